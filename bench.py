@@ -1,0 +1,424 @@
+"""Throughput of the fixed-background GRHD operator on B200.
+
+Workload (default): Kerr-Schild torus, M = 1, spin 0.9, 256^3 cells on
+[-40, 40]^3, ideal gas Gamma = 5/3, constant-ell torus (inner edge 6M,
+pressure maximum at 12M, rho_peak 1) with a seeded 1e-3 relative density
+perturbation, atmosphere rho_floor 1e-10 / pressure_floor 1e-12 /
+v^2 cap 0.8, MUSCL-MC (theta 2) + HLLE, excision r < 1.5, classic RK4,
+CFL 0.25, FP64.  A step is one RK4 step of the whole grid (4 RHS
+evaluations, 4 stage combinations with post-stage con2prim/atmosphere, the
+CFL reduction).  Metric: cell-updates/s (interior cells x steps / time).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one process per GPU) every rank advances its own
+replica of the grid (no data-path collective); value = all ranks' cell
+updates / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_CELLS = 256
+HALF_WIDTH = 40.0
+SPIN = 0.9
+GAMMA = 5.0 / 3.0
+CFL = 0.25
+SEED = 20261203 + 1
+BYTES_PER_CELL_UPDATE = 720   # RK4, FP64 state: 440 B read + 280 B write
+BYTES_PER_RHS_CELL = 80       # one RHS: 5 doubles read + 5 written
+METRIC = "GRHD cell-updates/s (RK4 step, KS torus a=0.9, 256^3, FP64)"
+
+
+def workload_config(n):
+    return {
+        "workload": f"kerr_schild_torus_a0.9_{n}^3_rk4_fp64",
+        "grid": [n, n, n], "domain": [-HALF_WIDTH, HALF_WIDTH],
+        "background": "KerrSchild M=1 a=0.9", "eos_gamma": GAMMA,
+        "torus": {"inner_radius": 6.0, "pressure_max_radius": 12.0,
+                  "rho_peak": 1.0, "density_perturbation": 1e-3,
+                  "seed": SEED},
+        "atmosphere": {"rho_floor": 1e-10, "pressure_floor": 1e-12,
+                       "max_velocity_squared": 0.8},
+        "reconstruction": "MUSCL-MC theta=2", "riemann": "HLLE",
+        "integrator": "RK4", "cfl": CFL, "excision_radius": 1.5,
+        "l2": "inputs larger than L2 (state 1.5 GB per grid)",
+    }
+
+
+# ----------------------------------------------------------------- GPU arm
+
+
+def make_operator(G, n):
+    dx = 2.0 * HALF_WIDTH / n
+    c = 0.5 * n * dx
+    return G.TimeDependentFixedBGLevelDataFiniteVolumeOperator(
+        G.IdealGasEOS(GAMMA), G.KerrSchild(mass=1.0, spin=SPIN, dx=dx), dx,
+        (c, c, c), G.AtmosphereOptions(1e-10, 1e-12, 0.8), 2.0, True,
+        G.RecoveryOptions(80, 1e-12, 1e-12, 0.8), True, False, 1e-3, 1.5)
+
+
+def build_state(G, op, n, device):
+    lv = G.LevelBox.cube(n, device=device)
+    op.fill_torus(lv, inner_radius=6.0, pressure_max_radius=12.0,
+                  rho_peak=1.0, max_velocity_squared=0.8)
+    op.perturb_density(lv, 1e-3, SEED)
+    op.recover_primitives(lv)
+    return lv
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,"
+              "clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu),
+                 f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                 "-lms", "200"], stdout=open(self.path, "w"),
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or not self.path:
+            return None
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm = float(parts[1].split()[0])
+                smax = float(parts[2].split()[0])
+            except ValueError:
+                continue
+            rows.append((sm, smax, parts[5:9]))
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows
+                          for i in range(4) if r[i].lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows),
+                "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import grdzhadzha_b200 as G
+
+    device = f"cuda:{local_rank}"
+    torch.cuda.set_device(local_rank)
+    n = args.n
+    op = make_operator(G, n)
+    lv = build_state(G, op, n, device)
+    cells = lv.num_cells
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+
+    def step(t):
+        dt = op.compute_stable_dt(lv, cfl=CFL, time=t)
+        op.advance_rk4(lv, time=t, dt=dt)
+        return t + dt
+
+    t = 0.0
+    for _ in range(args.warmup):
+        t = step(t)
+    torch.cuda.synchronize()
+    if dist:
+        tdist.barrier()
+    op.profile(True)
+    op.profile_read()
+    launches0 = op.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(args.steps):
+            t = step(t)
+        ev1.record()
+        torch.cuda.synchronize()
+    if dist:
+        tdist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches = op.launch_count() - launches0
+    prof = op.profile_read()
+    op.profile(False)
+    if dist:
+        x = torch.tensor([ms], dtype=torch.float64, device=device)
+        tdist.all_reduce(x, op=tdist.ReduceOp.MAX)
+        ms = float(x.item())
+    value = cells * args.steps * world / (ms / 1e3)
+
+    # ---- end to end through the API with host buffers ----
+    host_in = torch.empty_like(lv.state, device="cpu").pin_memory()
+    host_out = torch.empty_like(lv.state, device="cpu").pin_memory()
+    host_in.copy_(lv.state)
+    e2e_steps = max(1, min(args.steps, 5))
+    torch.cuda.synchronize()
+    if dist:
+        tdist.barrier()
+    ev0.record()
+    for _ in range(e2e_steps):
+        lv.state.copy_(host_in, non_blocking=True)
+        t = step(t)
+        host_out.copy_(lv.state, non_blocking=True)
+        torch.cuda.synchronize()
+        host_in, host_out = host_out, host_in
+    ev1.record()
+    torch.cuda.synchronize()
+    e2e_ms = ev0.elapsed_time(ev1)
+    if dist:
+        x = torch.tensor([e2e_ms], dtype=torch.float64, device=device)
+        tdist.all_reduce(x, op=tdist.ReduceOp.MAX)
+        e2e_ms = float(x.item())
+        tdist.barrier()
+    state_bytes = lv.state.numel() * lv.state.element_size()
+    e2e = {"value": cells * e2e_steps * world / (e2e_ms / 1e3),
+           "unit": "cell-updates/s", "h2d_bytes_per_step": state_bytes,
+           "d2h_bytes_per_step": state_bytes, "steps": e2e_steps}
+
+    # ---- roofline of the dominant kernel ----
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    dom = max(prof, key=lambda k: prof[k][0])
+    dom_ms, dom_n = prof[dom]
+    per_launch_cells = {"faces": cells, "cells": cells, "ghosts": cells,
+                        "stage": cells, "cfl": cells}[dom]
+    per_cell_bytes = {"faces": BYTES_PER_RHS_CELL,
+                      "cells": BYTES_PER_RHS_CELL,
+                      "ghosts": BYTES_PER_RHS_CELL,
+                      "stage": 200, "cfl": 40}[dom]
+    alg_bytes = per_launch_cells * per_cell_bytes
+    achieved = alg_bytes / (dom_ms / max(dom_n, 1) / 1e3) / 1e9
+    # DRAM traffic per launch from the committed ncu capture of the same
+    # kernel; a capture on a smaller grid is scaled by the cell count
+    traffic, traffic_note = None, None
+    try:
+        tr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        if tr.get("kernel_class") == dom:
+            g = int(tr["grid"])
+            traffic = tr["dram_bytes_per_launch"] * (n / g) ** 3
+            traffic_note = (f"ncu capture at {g}^3 scaled by cells"
+                            if g != n else "ncu capture")
+    except (OSError, ValueError, KeyError):
+        pass
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved,
+                "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": traffic,
+                "traffic_source": traffic_note, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": alg_bytes,
+                "avg_launch_ms": dom_ms / max(dom_n, 1),
+                "step_frac_of_hbm_roofline":
+                    value / world * BYTES_PER_CELL_UPDATE / 1e9 / hbm_peak}
+    kernel_ms = {k: {"ms_total": v[0], "launches": v[1]}
+                 for k, v in prof.items()}
+    return {"value": value, "ms": ms, "e2e": e2e, "roofline": roofline,
+            "clocks": clk.summary(), "launches": launches,
+            "kernel_ms": kernel_ms, "state": lv, "op": op}
+
+
+# ------------------------------------------------------------ CPU oracle
+
+
+class CpuBaseline:
+    """The oracle (the reference's algorithm, per-box structure, one z-slab
+    box per host thread) on the same workload: a mid-plane z-slab of the
+    256^3 grid, nz = min(256, 16 x threads) planes, so each box is at
+    least 16 planes thick.  Its state is built by the oracle itself (torus
+    + numpy-seeded 1e-3 perturbation + recovery)."""
+
+    def __init__(self, threads):
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import numpy as np
+        import oracle_lib as O
+
+        self.O = O
+        self.threads = threads
+        O.set_threads(threads)
+        n = N_CELLS
+        dx = 2.0 * HALF_WIDTH / n
+        c = 0.5 * n * dx
+        p = O.default_params(background=O.BG_KERR_SCHILD, ks_mass=1.0,
+                             ks_spin=SPIN, gamma=GAMMA, dx=dx,
+                             center=(c, c, c), atmo_rho_floor=1e-10,
+                             atmo_pressure_floor=1e-12,
+                             atmo_max_velocity_squared=0.8,
+                             rec_max_iterations=80,
+                             rec_max_velocity_squared=0.8, limiter_theta=2.0,
+                             excision_radius=1.5)
+        nz = min(n, 16 * threads)
+        box = O.Box()
+        z0 = n // 2 - nz // 2
+        for d, (lo, hi) in enumerate(((0, n - 1), (0, n - 1),
+                                      (z0, z0 + nz - 1))):
+            box.lo[d], box.hi[d] = lo, hi
+            box.glo[d], box.ghi[d] = lo - 2, hi + 2
+            box.dlo[d], box.dhi[d] = 0, n - 1
+        box.comp_stride = (n + 4) * (n + 4) * (nz + 4)
+        s = O.new_state(box)
+        cfg = O.torus_config(total_mass=1.0, inner_radius=6.0,
+                             pressure_max_radius=12.0, rho_peak=1.0,
+                             max_velocity_squared=0.8)
+        tp = O.make_torus(p, cfg, box, 0.0)
+        O.fill_torus(p, cfg, tp, box, s, 0.0)
+        rng = np.random.default_rng(SEED)
+        V = O.state_view(box, s)
+        V[O.RHO] *= 1.0 + 1e-3 * rng.uniform(-1, 1, V[O.RHO].shape)
+        V[O.EPS] = V[O.PRESS] / ((GAMMA - 1.0) * V[O.RHO])
+        O.fill_conserved_from_primitives(p, box, s)
+        O.recover_primitives(p, box, s)
+        self.p, self.box, self.s, self.nz = p, box, s, nz
+        self.cells = n * n * nz
+        self.desc = (f"one RHS evaluation of the oracle (the reference's "
+                     f"per-box algorithm, {threads} z-slab boxes of "
+                     f"{nz // threads}+ planes, one thread each) over the "
+                     f"{n}x{n}x{nz} mid-plane slab of the {n}^3 grid; "
+                     f"RK4 step = 4 RHS evaluations")
+
+    def sample(self):
+        """RK4-equivalent cell-updates/s of one RHS evaluation."""
+        t0 = time.perf_counter()
+        self.O.compute_rhs_slabs(self.p, self.box, self.s, self.threads)
+        el = time.perf_counter() - t0
+        return self.cells / el / 4.0
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# -------------------------------------------------------------------- main
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=N_CELLS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        threads = host_threads()
+        cb = CpuBaseline(threads)
+        samples = []
+        for i in range(args.warmup + args.steps):
+            rate = cb.sample()
+            if i >= args.warmup:
+                samples.append(rate)
+        value = statistics.median(samples)
+        sample_desc = cb.desc
+        line = {
+            "impl": "reference", "metric": METRIC, "value": value,
+            "unit": "cell-updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": N_CELLS ** 3 / value * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": workload_config(N_CELLS),
+            "cpu_baseline": {"value": value, "unit": "cell-updates/s",
+                             "cores": threads, "kind": "port",
+                             "sample": sample_desc},
+            "e2e": {"value": value, "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return
+
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                 device_id=torch.device(f"cuda:{local_rank}"))
+    res = run_ours(args, rank, world, local_rank)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = host_threads()
+        cb = CpuBaseline(threads)
+        rate = max(cb.sample() for _ in range(2))
+        cpu = {"value": rate, "unit": "cell-updates/s", "cores": threads,
+               "kind": "port", "sample": cb.desc}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": res["value"],
+            "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": res["ms"] / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded torus initial data generated on the "
+                    "device)",
+            "config": dict(workload_config(args.n),
+                           parallelism=f"replicas x{world}"),
+            "e2e": res["e2e"], "roofline": res["roofline"],
+            "cpu_baseline": cpu, "clocks": res["clocks"],
+            "gpu_launches": res["launches"], "kernel_ms": res["kernel_ms"],
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as tdist
+        tdist.barrier()
+        tdist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,13 @@
+"""B200-native fixed-background Valencia GRHD operator (GRDzhadzha's
+Source/Matter/GRHD fixed-background path) over a C ABI."""
+from .operator import (  # noqa: F401
+    AtmosphereOptions,
+    CircularBinaryPN,
+    FixedBGLevelDataFiniteVolumeOperator,
+    IdealGasEOS,
+    KerrSchild,
+    LevelBox,
+    RecoveryOptions,
+    TimeDependentFixedBGLevelDataFiniteVolumeOperator,
+)
+from ._lib import GRHDError, InvalidArgument  # noqa: F401

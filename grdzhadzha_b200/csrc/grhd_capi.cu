@@ -1,0 +1,951 @@
+// grhd_capi.cu -- the extern "C" boundary (include/grhd_b200.h): context,
+// scratch management, status/error reporting and the operator methods of
+// the reference's FixedBGLevelDataFiniteVolumeOperator /
+// TimeDependentFixedBGLevelDataFiniteVolumeOperator
+// (Source/Matter/GRHD/FixedBGFArrayBoxFiniteVolume.hpp:446-830).
+#include "grhd_b200.h"
+#include "grhd_initial_data.cuh"
+#include "grhd_kernels.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+using namespace grhd;
+
+struct grhd_ctx
+{
+    grhd_params params;
+    Options opt;
+    int device;
+    // scratch, grown on demand
+    double *prim = nullptr;  // 5 comps over the ghosted box
+    size_t prim_cap = 0;     // doubles
+    double *src = nullptr;   // 5 comps over the interior
+    double *kbuf = nullptr;  // 5 comps over the interior
+    double *acc = nullptr;   // 5 comps over the interior
+    size_t int_cap = 0;      // doubles per interior buffer
+    double *stage = nullptr; // 11 comps over the ghosted box
+    size_t stage_cap = 0;
+    DevStatus *status = nullptr;   // device
+    DevStatus *status_h = nullptr; // pinned host mirror
+    double *probe = nullptr;       // device scalars: probe + torus setup
+    int *flag = nullptr;           // device flag (initial-data failures)
+    int zchunk = 32;
+    grhd_error last_error;
+    // instrumentation
+    long long launches = 0;
+    bool prof_on = false;
+    struct ProfRec
+    {
+        cudaEvent_t a, b;
+        int cls;
+    };
+    std::vector<ProfRec> prof_pending;
+    std::vector<cudaEvent_t> event_pool;
+};
+
+namespace {
+
+const unsigned long long kNoError = ~0ull;
+
+cudaEvent_t take_event(grhd_ctx *ctx)
+{
+    if (!ctx->event_pool.empty())
+    {
+        cudaEvent_t e = ctx->event_pool.back();
+        ctx->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Brackets one kernel launch: counts it and, when profiling is on, records
+// a pair of events on its stream.
+struct Timed
+{
+    grhd_ctx *ctx;
+    cudaStream_t s;
+    grhd_ctx::ProfRec rec;
+    Timed(grhd_ctx *c, int cls, cudaStream_t st) : ctx(c), s(st)
+    {
+        ++ctx->launches;
+        rec.cls = cls;
+        rec.a = rec.b = nullptr;
+        if (ctx->prof_on)
+        {
+            rec.a = take_event(ctx);
+            rec.b = take_event(ctx);
+            cudaEventRecord(rec.a, s);
+        }
+    }
+    ~Timed()
+    {
+        if (rec.a)
+        {
+            cudaEventRecord(rec.b, s);
+            ctx->prof_pending.push_back(rec);
+        }
+    }
+};
+
+int set_error(grhd_ctx *ctx, int status, int where, const int cell[3],
+              double residual, const char *msg)
+{
+    grhd_error &e = ctx->last_error;
+    e.status = status;
+    e.where = where;
+    for (int d = 0; d < 3; ++d)
+        e.cell[d] = cell ? cell[d] : 0;
+    e.residual = residual;
+    std::snprintf(e.message, sizeof(e.message), "%s", msg ? msg : "");
+    return status;
+}
+
+int cuda_error(grhd_ctx *ctx, cudaError_t err, const char *what)
+{
+    char buf[256];
+    std::snprintf(buf, sizeof(buf), "CUDA error in %s: %s", what,
+                  cudaGetErrorString(err));
+    return set_error(ctx, GRHD_ERR_CUDA, GRHD_WHERE_NONE, nullptr, 0.0, buf);
+}
+
+#define GRHD_CUDA(ctx, call)                                                  \
+    do                                                                        \
+    {                                                                         \
+        cudaError_t e_ = (call);                                              \
+        if (e_ != cudaSuccess)                                                \
+            return cuda_error((ctx), e_, #call);                              \
+    } while (0)
+
+Options make_options(const grhd_params &p)
+{
+    Options o;
+    o.G = p.adiabatic_index;
+    o.rho_floor = p.rho_floor;
+    o.p_floor = p.pressure_floor;
+    o.atmo_vmax2 = p.max_velocity_squared;
+    o.src_atmo_factor = p.metric_source_atmosphere_factor;
+    o.rec_maxit = p.recovery_max_iterations;
+    o.rec_tol = p.recovery_tolerance;
+    o.rec_pfloor = p.recovery_pressure_floor;
+    o.rec_vmax2 = p.recovery_max_velocity_squared;
+    o.theta = p.limiter_theta;
+    o.use_recon = p.use_reconstruction;
+    o.use_src = p.use_static_metric_sources;
+    o.use_vol = p.use_metric_volume_time_sources;
+    o.excision_radius = p.excision_radius;
+    o.dx = p.dx;
+    for (int d = 0; d < 3; ++d)
+        o.center[d] = p.center[d];
+    return o;
+}
+
+// CircularBinaryPN::compute_state (:219-250) at operator time t; the
+// reference's background factory adds t to params.time
+// (Tests/GRHDFixedBGTest/GRHDFixedBGTest.cpp:440-445).
+void pn_state(const grhd_params &p, double t, double p1[3], double p2[3],
+              double v1[3], double v2[3])
+{
+    const double total = p.pn_mass_1 + p.pn_mass_2;
+    const double omega =
+        p.pn_angular_velocity != 0.0
+            ? p.pn_angular_velocity
+            : std::sqrt(total / (p.pn_separation * p.pn_separation *
+                                 p.pn_separation));
+    const double phase = p.pn_phase + omega * (p.pn_time + t);
+    const double c = std::cos(phase), s = std::sin(phase);
+    const double r1 = p.pn_mass_2 / total * p.pn_separation;
+    const double r2 = p.pn_mass_1 / total * p.pn_separation;
+    for (int i = 0; i < 3; ++i)
+        p1[i] = p2[i] = v1[i] = v2[i] = 0.0;
+    p1[0] = r1 * c;
+    p1[1] = r1 * s;
+    p2[0] = -r2 * c;
+    p2[1] = -r2 * s;
+    v1[0] = -omega * r1 * s;
+    v1[1] = omega * r1 * c;
+    v2[0] = omega * r2 * s;
+    v2[1] = -omega * r2 * c;
+}
+
+Background make_background(const grhd_params &p, double t)
+{
+    Background bg;
+    std::memset(&bg, 0, sizeof(bg));
+    bg.kind = p.background;
+    bg.M = p.ks_mass;
+    bg.a = p.ks_spin;
+    if (p.background == GRHD_BG_BINARY_PN)
+    {
+        bg.m1 = p.pn_mass_1;
+        bg.m2 = p.pn_mass_2;
+        bg.soft2 = p.pn_softening_radius * p.pn_softening_radius;
+        pn_state(p, t, bg.p1, bg.p2, bg.v1, bg.v2);
+        // fixed_background_log_sqrt_det_time_derivative, :616-631
+        const double h = std::fmax(p.metric_time_derivative_step, 1.0e-12);
+        bg.fd_h = h;
+        double vv1[3], vv2[3];
+        pn_state(p, t + h, bg.p1p, bg.p2p, vv1, vv2);
+        pn_state(p, t - h, bg.p1m, bg.p2m, vv1, vv2);
+    }
+    return bg;
+}
+
+bool valid_box(const grhd_box *b)
+{
+    if (!b || b->ghost < 2)
+        return false;
+    for (int d = 0; d < 3; ++d)
+        if (b->lo[d] > b->hi[d] || b->domain_lo[d] > b->domain_hi[d])
+            return false;
+    return true;
+}
+
+BoxDev make_box(const grhd_box *b, int64_t state_cs)
+{
+    BoxDev x;
+    for (int d = 0; d < 3; ++d)
+    {
+        x.lo[d] = b->lo[d];
+        x.hi[d] = b->hi[d];
+        x.glo[d] = b->lo[d] - b->ghost;
+        x.ghi[d] = b->hi[d] + b->ghost;
+        x.dlo[d] = b->domain_lo[d];
+        x.dhi[d] = b->domain_hi[d];
+        x.gn[d] = x.ghi[d] - x.glo[d] + 1;
+        x.in[d] = x.hi[d] - x.lo[d] + 1;
+    }
+    x.cs = state_cs;
+    x.rcs = x.ivol();
+    x.pcs = x.gvol();
+    return x;
+}
+
+int check_strides(grhd_ctx *ctx, const BoxDev &b, int64_t state_cs,
+                  int64_t rhs_cs)
+{
+    const int cell[3] = {0, 0, 0};
+    if (state_cs < b.gvol())
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, cell, 0.0,
+                         "state component stride is smaller than the "
+                         "ghosted box volume");
+    if (rhs_cs >= 0 && rhs_cs < b.ivol())
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, cell, 0.0,
+                         "rhs component stride is smaller than the interior "
+                         "box volume");
+    return GRHD_OK;
+}
+
+int grow(grhd_ctx *ctx, double **ptr, size_t *cap, size_t need)
+{
+    if (*cap >= need)
+        return GRHD_OK;
+    if (*ptr)
+        cudaFree(*ptr);
+    *ptr = nullptr;
+    *cap = 0;
+    GRHD_CUDA(ctx, cudaMalloc((void **)ptr, need * sizeof(double)));
+    *cap = need;
+    return GRHD_OK;
+}
+
+int ensure_scratch(grhd_ctx *ctx, const BoxDev &b, bool need_stage)
+{
+    int st = grow(ctx, &ctx->prim, &ctx->prim_cap, 5 * (size_t)b.gvol());
+    if (st)
+        return st;
+    const size_t ni = 5 * (size_t)b.ivol();
+    if (ctx->int_cap < ni)
+    {
+        size_t c1 = ctx->int_cap, c2 = ctx->int_cap, c3 = ctx->int_cap;
+        if ((st = grow(ctx, &ctx->src, &c1, ni)) ||
+            (st = grow(ctx, &ctx->kbuf, &c2, ni)) ||
+            (st = grow(ctx, &ctx->acc, &c3, ni)))
+            return st;
+        ctx->int_cap = ni;
+    }
+    if (need_stage)
+        st = grow(ctx, &ctx->stage, &ctx->stage_cap,
+                  kStateComps * (size_t)b.gvol());
+    return st;
+}
+
+int reset_status(grhd_ctx *ctx, cudaStream_t s)
+{
+    DevStatus init;
+    init.err_key = kNoError;
+    for (int q = 0; q < 4; ++q)
+        init.counts[q] = 0;
+    init.maxinv_bits = 0;
+    *ctx->status_h = init;
+    GRHD_CUDA(ctx, cudaMemcpyAsync(ctx->status, ctx->status_h,
+                                   sizeof(DevStatus), cudaMemcpyHostToDevice,
+                                   s));
+    return GRHD_OK;
+}
+
+// Reads the device status back (synchronising the stream) and converts a
+// recorded recovery failure into the reference's exception data.
+int finish_status(grhd_ctx *ctx, const BoxDev &b, const double *state,
+                  const Background &bg, cudaStream_t s)
+{
+    GRHD_CUDA(ctx, cudaGetLastError());
+    GRHD_CUDA(ctx, cudaMemcpyAsync(ctx->status_h, ctx->status,
+                                   sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                                   s));
+    GRHD_CUDA(ctx, cudaStreamSynchronize(s));
+    const unsigned long long key = ctx->status_h->err_key;
+    if (key == kNoError)
+        return GRHD_OK;
+    const int where = (int)(key >> 56);
+    const int64_t order = (int64_t)(key & ((1ull << 56) - 1));
+    int cell[3];
+    int probe[3];
+    if (where == GRHD_WHERE_CFL)
+    {
+        cell[0] = b.lo[0] + (int)(order % b.in[0]);
+        cell[1] = b.lo[1] + (int)((order / b.in[0]) % b.in[1]);
+        cell[2] = b.lo[2] + (int)(order / ((int64_t)b.in[0] * b.in[1]));
+    }
+    else
+    {
+        cell[0] = b.glo[0] + (int)(order % b.gn[0]);
+        cell[1] = b.glo[1] + (int)((order / b.gn[0]) % b.gn[1]);
+        cell[2] = b.glo[2] + (int)(order / ((int64_t)b.gn[0] * b.gn[1]));
+    }
+    for (int d = 0; d < 3; ++d)
+        probe[d] = cell[d];
+    if (where == GRHD_WHERE_OUTFLOW_SOURCE)
+    {
+        // the failing con2prim is at the clamped interior source cell
+        for (int d = 0; d < 3; ++d)
+        {
+            if (cell[d] < b.dlo[d])
+                probe[d] = b.lo[d];
+            else if (cell[d] > b.dhi[d])
+                probe[d] = b.hi[d];
+        }
+    }
+    double residual = 0.0;
+    launch_residual_probe(state, b, bg, ctx->opt, probe[0], probe[1],
+                          probe[2], ctx->probe, s);
+    GRHD_CUDA(ctx, cudaMemcpyAsync(&residual, ctx->probe, sizeof(double),
+                                   cudaMemcpyDeviceToHost, s));
+    GRHD_CUDA(ctx, cudaStreamSynchronize(s));
+    char msg[256];
+    const char *what =
+        where == GRHD_WHERE_OUTFLOW_SOURCE
+            ? "GRHD primitive recovery failed at outflow source (%d,%d,%d) "
+              "while filling fixed-background boundary, residual %g"
+        : where == GRHD_WHERE_CFL
+            ? "GRHD primitive recovery failed at (%d,%d,%d) while computing "
+              "fixed-background CFL speed, residual %g"
+            : "GRHD primitive recovery failed at (%d,%d,%d) with residual %g "
+              "on fixed background";
+    std::snprintf(msg, sizeof(msg), what, probe[0], probe[1], probe[2],
+                  residual);
+    return set_error(ctx, GRHD_ERR_RECOVERY, where, probe, residual, msg);
+}
+
+void read_diag(const grhd_ctx *ctx, grhd_diagnostics *d)
+{
+    if (!d)
+        return;
+    d->num_cells += (long long)ctx->status_h->counts[0];
+    d->num_failed_recoveries += (long long)ctx->status_h->counts[1];
+    d->num_floored_primitives += (long long)ctx->status_h->counts[2];
+    d->num_conserved_resets += (long long)ctx->status_h->counts[3];
+}
+
+// One RHS evaluation on the device (no synchronisation).
+void enqueue_rhs(grhd_ctx *ctx, double *rhs, double *state, const BoxDev &b,
+                 const Background &bg, const double inv_dx[3], cudaStream_t s)
+{
+    {
+        Timed t_(ctx, GRHD_K_GHOSTS, s);
+        launch_fill_ghosts(state, b, bg, ctx->opt, ctx->status, s);
+    }
+    {
+        Timed t_(ctx, GRHD_K_CELLS, s);
+        launch_cells(state, ctx->prim, ctx->src, b, bg, ctx->opt, ctx->status,
+                     s);
+    }
+    {
+        Timed t_(ctx, GRHD_K_FACES, s);
+        launch_faces(ctx->prim, ctx->src, rhs, b, bg, ctx->opt, inv_dx,
+                     ctx->zchunk, s);
+    }
+}
+
+bool box_is_domain(const grhd_box *b)
+{
+    for (int d = 0; d < 3; ++d)
+        if (b->lo[d] != b->domain_lo[d] || b->hi[d] != b->domain_hi[d])
+            return false;
+    return true;
+}
+
+int common_checks(grhd_ctx *ctx, const void *state, const grhd_box *box)
+{
+    const int cell[3] = {0, 0, 0};
+    if (!ctx)
+        return GRHD_ERR_INVALID_ARG;
+    std::memset(&ctx->last_error, 0, sizeof(ctx->last_error));
+    if (!state || !valid_box(box))
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, cell, 0.0,
+                         "invalid state pointer or box");
+    if (!(ctx->params.dx > 0.0))
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, cell, 0.0,
+                         "GRHD grid spacing must be positive");
+    GRHD_CUDA(ctx, cudaSetDevice(ctx->device));
+    return GRHD_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int grhd_abi_version(void) { return GRHD_B200_ABI_VERSION; }
+
+void grhd_default_params(grhd_params *p)
+{
+    std::memset(p, 0, sizeof(*p));
+    p->background = GRHD_BG_KERR_SCHILD;
+    p->ks_mass = 1.0;
+    p->ks_spin = 0.0;
+    p->pn_mass_1 = 0.5;
+    p->pn_mass_2 = 0.5;
+    p->pn_separation = 10.0;
+    p->pn_angular_velocity = 0.0;
+    p->pn_phase = 0.0;
+    p->pn_time = 0.0;
+    p->pn_softening_radius = 0.5;
+    p->adiabatic_index = 5.0 / 3.0;
+    p->dx = 1.0;
+    p->rho_floor = 1.0e-12;
+    p->pressure_floor = 1.0e-12;
+    p->max_velocity_squared = 1.0 - 1.0e-12;
+    p->metric_source_atmosphere_factor = 1.0 + 1.0e-12;
+    p->recovery_max_iterations = 50;
+    p->recovery_tolerance = 1.0e-12;
+    p->recovery_pressure_floor = 1.0e-12;
+    p->recovery_max_velocity_squared = 1.0 - 1.0e-12;
+    p->limiter_theta = 1.5;
+    p->use_reconstruction = 1;
+    p->use_static_metric_sources = 1;
+    p->use_metric_volume_time_sources = 0;
+    p->metric_time_derivative_step = 1.0e-3;
+    p->excision_radius = 0.0;
+}
+
+const char *grhd_status_string(int status)
+{
+    switch (status)
+    {
+    case GRHD_OK:
+        return "ok";
+    case GRHD_ERR_RECOVERY:
+        return "primitive recovery failed";
+    case GRHD_ERR_INVALID_ARG:
+        return "invalid argument";
+    case GRHD_ERR_CUDA:
+        return "CUDA error";
+    case GRHD_ERR_SETUP:
+        return "setup failed";
+    default:
+        return "unknown status";
+    }
+}
+
+int grhd_create(const grhd_params *params, grhd_ctx **out)
+{
+    if (!params || !out)
+        return GRHD_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (!(params->dx > 0.0))
+        return GRHD_ERR_INVALID_ARG;
+    if (params->background == GRHD_BG_KERR_SCHILD &&
+        (params->ks_spin > params->ks_mass ||
+         params->ks_spin < -params->ks_mass))
+        return GRHD_ERR_INVALID_ARG; // KerrSchild.hpp:81-90
+    if (params->background == GRHD_BG_BINARY_PN &&
+        (params->pn_mass_1 <= 0.0 || params->pn_mass_2 <= 0.0 ||
+         params->pn_separation <= 0.0 || params->pn_softening_radius < 0.0))
+        return GRHD_ERR_INVALID_ARG; // CircularBinaryPN.hpp:49-57
+    if (params->background != GRHD_BG_KERR_SCHILD &&
+        params->background != GRHD_BG_BINARY_PN)
+        return GRHD_ERR_INVALID_ARG;
+    grhd_ctx *ctx = new (std::nothrow) grhd_ctx();
+    if (!ctx)
+        return GRHD_ERR_SETUP;
+    ctx->params = *params;
+    ctx->opt = make_options(*params);
+    std::memset(&ctx->last_error, 0, sizeof(ctx->last_error));
+    if (cudaGetDevice(&ctx->device) != cudaSuccess ||
+        configure_kernels() != cudaSuccess ||
+        cudaMalloc((void **)&ctx->status, sizeof(DevStatus)) != cudaSuccess ||
+        cudaMallocHost((void **)&ctx->status_h, sizeof(DevStatus)) !=
+            cudaSuccess ||
+        cudaMalloc((void **)&ctx->probe, 8 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc((void **)&ctx->flag, sizeof(int)) != cudaSuccess)
+    {
+        grhd_destroy(ctx);
+        return GRHD_ERR_CUDA;
+    }
+    *out = ctx;
+    return GRHD_OK;
+}
+
+void grhd_destroy(grhd_ctx *ctx)
+{
+    if (!ctx)
+        return;
+    cudaFree(ctx->prim);
+    cudaFree(ctx->src);
+    cudaFree(ctx->kbuf);
+    cudaFree(ctx->acc);
+    cudaFree(ctx->stage);
+    cudaFree(ctx->status);
+    cudaFree(ctx->probe);
+    cudaFree(ctx->flag);
+    if (ctx->status_h)
+        cudaFreeHost(ctx->status_h);
+    for (auto &r : ctx->prof_pending)
+    {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (cudaEvent_t e : ctx->event_pool)
+        cudaEventDestroy(e);
+    delete ctx;
+}
+
+int grhd_last_error(const grhd_ctx *ctx, grhd_error *out)
+{
+    if (!ctx || !out)
+        return GRHD_ERR_INVALID_ARG;
+    *out = ctx->last_error;
+    return GRHD_OK;
+}
+
+int grhd_compute_rhs(grhd_ctx *ctx, double *rhs, int64_t rhs_cs,
+                     double *state, int64_t state_cs, const grhd_box *box,
+                     const double inverse_dx[3], double time, void *stream)
+{
+    int st = common_checks(ctx, state, box);
+    if (st)
+        return st;
+    if (!rhs || !inverse_dx)
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "null rhs or inverse_dx");
+    cudaStream_t s = (cudaStream_t)stream;
+    const BoxDev b = make_box(box, state_cs);
+    if ((st = check_strides(ctx, b, state_cs, rhs_cs)) ||
+        (st = ensure_scratch(ctx, b, false)) || (st = reset_status(ctx, s)))
+        return st;
+    const Background bg = make_background(ctx->params, time);
+    // the face kernel writes with the interior-volume stride; a caller
+    // stride that differs goes through the k scratch buffer
+    if (rhs_cs == b.ivol())
+        enqueue_rhs(ctx, rhs, state, b, bg, inverse_dx, s);
+    else
+    {
+        enqueue_rhs(ctx, ctx->kbuf, state, b, bg, inverse_dx, s);
+        for (int c = 0; c < 5; ++c)
+            GRHD_CUDA(ctx, cudaMemcpyAsync(rhs + c * rhs_cs,
+                                           ctx->kbuf + c * b.ivol(),
+                                           b.ivol() * sizeof(double),
+                                           cudaMemcpyDeviceToDevice, s));
+    }
+    return finish_status(ctx, b, state, bg, s);
+}
+
+int grhd_recover_primitives(grhd_ctx *ctx, double *state, int64_t state_cs,
+                            const grhd_box *box, double time,
+                            grhd_diagnostics *diag, void *stream)
+{
+    int st = common_checks(ctx, state, box);
+    if (st)
+        return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    const BoxDev b = make_box(box, state_cs);
+    if ((st = check_strides(ctx, b, state_cs, -1)) ||
+        (st = reset_status(ctx, s)))
+        return st;
+    const Background bg = make_background(ctx->params, time);
+    {
+        Timed t_(ctx, GRHD_K_STAGE, s);
+        launch_recover(state, b, bg, ctx->opt, ctx->status, s);
+    }
+    st = finish_status(ctx, b, state, bg, s);
+    read_diag(ctx, diag);
+    return st;
+}
+
+int grhd_update_conserved(grhd_ctx *ctx, double *state, int64_t state_cs,
+                          const double *rhs, int64_t rhs_cs,
+                          const grhd_box *box, double dt,
+                          double recovery_time, int recover,
+                          grhd_diagnostics *diag, void *stream)
+{
+    int st = common_checks(ctx, state, box);
+    if (st)
+        return st;
+    if (!rhs)
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "null rhs");
+    cudaStream_t s = (cudaStream_t)stream;
+    BoxDev b = make_box(box, state_cs);
+    b.rcs = rhs_cs;
+    if ((st = check_strides(ctx, b, state_cs, rhs_cs)) ||
+        (st = reset_status(ctx, s)))
+        return st;
+    const Background bg = make_background(ctx->params, recovery_time);
+    {
+        Timed t_(ctx, GRHD_K_STAGE, s);
+        launch_update(state, b.cs, state, b.cs, rhs, b, bg, ctx->opt, dt,
+                      recover, ctx->status, s);
+    }
+    st = finish_status(ctx, b, state, bg, s);
+    read_diag(ctx, diag);
+    return st;
+}
+
+int grhd_compute_max_inverse_dt(grhd_ctx *ctx, const double *state,
+                                int64_t state_cs, const grhd_box *box,
+                                const double inverse_dx[3], double time,
+                                double *out, void *stream)
+{
+    int st = common_checks(ctx, state, box);
+    if (st)
+        return st;
+    if (!out || !inverse_dx)
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "null output or inverse_dx");
+    cudaStream_t s = (cudaStream_t)stream;
+    const BoxDev b = make_box(box, state_cs);
+    if ((st = check_strides(ctx, b, state_cs, -1)) ||
+        (st = reset_status(ctx, s)))
+        return st;
+    const Background bg = make_background(ctx->params, time);
+    {
+        Timed t_(ctx, GRHD_K_CFL, s);
+        launch_max_inv_dt(state, b, bg, ctx->opt, inverse_dx, ctx->status, s);
+    }
+    st = finish_status(ctx, b, state, bg, s);
+    if (st)
+        return st;
+    double v;
+    const unsigned long long bits = ctx->status_h->maxinv_bits;
+    std::memcpy(&v, &bits, sizeof(v));
+    *out = v;
+    return GRHD_OK;
+}
+
+int grhd_compute_stable_dt(grhd_ctx *ctx, const double *state,
+                           int64_t state_cs, const grhd_box *box,
+                           const double inverse_dx[3], double cfl,
+                           double time, double *out, void *stream)
+{
+    if (ctx && !(cfl > 0.0))
+    {
+        std::memset(&ctx->last_error, 0, sizeof(ctx->last_error));
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "GRHD CFL number must be positive");
+    }
+    double m = 0.0;
+    int st = grhd_compute_max_inverse_dt(ctx, state, state_cs, box,
+                                         inverse_dx, time, &m, stream);
+    if (st)
+        return st;
+    *out = cfl / std::fmax(m, 1.0e-14);
+    return GRHD_OK;
+}
+
+int grhd_advance_ssprk2(grhd_ctx *ctx, double *state, int64_t state_cs,
+                        const grhd_box *box, const double inverse_dx[3],
+                        double time, double dt, grhd_diagnostics *diag,
+                        void *stream)
+{
+    int st = common_checks(ctx, state, box);
+    if (st)
+        return st;
+    if (!inverse_dx || !box_is_domain(box))
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "advance needs the box to cover the whole domain");
+    cudaStream_t s = (cudaStream_t)stream;
+    const BoxDev b = make_box(box, state_cs);
+    if ((st = check_strides(ctx, b, state_cs, -1)) ||
+        (st = ensure_scratch(ctx, b, true)) || (st = reset_status(ctx, s)))
+        return st;
+    BoxDev sb = b; // the stage buffer is packed: stride = ghosted volume
+    sb.cs = b.gvol();
+    const Background bg0 = make_background(ctx->params, time);
+    const Background bg1 = make_background(ctx->params, time + dt);
+    // rhs_initial = L(state); stage = state + dt rhs_initial, recovered
+    enqueue_rhs(ctx, ctx->kbuf, state, b, bg0, inverse_dx, s);
+    {
+        // stage interior from state (different strides): update kernel
+        // reads `state` with stride b.cs and writes the stage with sb.cs.
+        // Both are indexed by the ghosted linear index, so use a strided
+        // copy of the 11 components first, then update in place.
+        GRHD_CUDA(ctx, cudaMemcpy2DAsync(ctx->stage, sb.cs * sizeof(double),
+                                         state, b.cs * sizeof(double),
+                                         b.gvol() * sizeof(double),
+                                         kStateComps,
+                                         cudaMemcpyDeviceToDevice, s));
+    }
+    {
+        Timed t_(ctx, GRHD_K_STAGE, s);
+        launch_update(ctx->stage, sb.cs, ctx->stage, sb.cs, ctx->kbuf, sb,
+                      bg1, ctx->opt, dt, 1, ctx->status, s);
+    }
+    // rhs_stage = L(stage) at t + dt
+    enqueue_rhs(ctx, ctx->kbuf, ctx->stage, sb, bg1, inverse_dx, s);
+    {
+        Timed t_(ctx, GRHD_K_STAGE, s);
+        launch_ssprk2_combine(state, b.cs, ctx->stage, sb.cs, ctx->kbuf, b,
+                              bg1, ctx->opt, dt, ctx->status, s);
+    }
+    st = finish_status(ctx, b, state, bg0, s);
+    read_diag(ctx, diag);
+    return st;
+}
+
+int grhd_advance_rk4(grhd_ctx *ctx, double *state, int64_t state_cs,
+                     const grhd_box *box, const double inverse_dx[3],
+                     double time, double dt, grhd_diagnostics *diag,
+                     void *stream)
+{
+    int st = common_checks(ctx, state, box);
+    if (st)
+        return st;
+    if (!inverse_dx || !box_is_domain(box))
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "advance needs the box to cover the whole domain");
+    cudaStream_t s = (cudaStream_t)stream;
+    const BoxDev b = make_box(box, state_cs);
+    if ((st = check_strides(ctx, b, state_cs, -1)) ||
+        (st = ensure_scratch(ctx, b, true)) || (st = reset_status(ctx, s)))
+        return st;
+    BoxDev sb = b;
+    sb.cs = b.gvol();
+    const Background bgs[4] = {
+        make_background(ctx->params, time),
+        make_background(ctx->params, time + 0.5 * dt),
+        make_background(ctx->params, time + 0.5 * dt),
+        make_background(ctx->params, time + dt)};
+    const Background bg_rec[4] = {bgs[1], bgs[1], bgs[3], bgs[3]};
+    // the stage buffer starts as a copy of the state (its excised cells
+    // keep the frozen primitives)
+    GRHD_CUDA(ctx, cudaMemcpy2DAsync(ctx->stage, sb.cs * sizeof(double), state,
+                                     b.cs * sizeof(double),
+                                     b.gvol() * sizeof(double), kStateComps,
+                                     cudaMemcpyDeviceToDevice, s));
+    for (int stage = 0; stage < 4; ++stage)
+    {
+        if (stage == 0)
+            enqueue_rhs(ctx, ctx->kbuf, state, b, bgs[0], inverse_dx, s);
+        else
+            enqueue_rhs(ctx, ctx->kbuf, ctx->stage, sb, bgs[stage],
+                        inverse_dx, s);
+        // stages 0-2 write U^n + c dt k into the stage buffer; stage 3 writes
+        // U^{n+1} into the caller's state
+        Timed t_(ctx, GRHD_K_STAGE, s);
+        if (stage < 3)
+            launch_rk4_stage(state, b.cs, ctx->stage, sb.cs, ctx->kbuf,
+                             ctx->acc, b, bg_rec[stage], ctx->opt, stage, dt,
+                             ctx->status, s);
+        else
+            launch_rk4_stage(state, b.cs, state, b.cs, ctx->kbuf, ctx->acc, b,
+                             bg_rec[stage], ctx->opt, stage, dt, ctx->status,
+                             s);
+    }
+    st = finish_status(ctx, b, state, bgs[0], s);
+    read_diag(ctx, diag);
+    return st;
+}
+
+int grhd_eval_background(grhd_ctx *ctx, int64_t n, const double *xyz,
+                         double time, double *out, void *stream)
+{
+    if (!ctx || n < 0 || (n > 0 && (!xyz || !out)))
+        return GRHD_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Background bg = make_background(ctx->params, time);
+    launch_eval_background(n, xyz, bg, out, s);
+    GRHD_CUDA(ctx, cudaGetLastError());
+    GRHD_CUDA(ctx, cudaStreamSynchronize(s));
+    return GRHD_OK;
+}
+
+int grhd_eval_con2prim(grhd_ctx *ctx, int64_t n, const double *cons,
+                       const double *gUU, double *prim, int *ok,
+                       int *iterations, double *residual, void *stream)
+{
+    if (!ctx || n < 0 ||
+        (n > 0 && (!cons || !gUU || !prim || !ok || !iterations || !residual)))
+        return GRHD_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    launch_eval_con2prim(n, cons, gUU, ctx->opt, prim, ok, iterations,
+                         residual, s);
+    GRHD_CUDA(ctx, cudaGetLastError());
+    GRHD_CUDA(ctx, cudaStreamSynchronize(s));
+    return GRHD_OK;
+}
+
+void grhd_default_torus_config(grhd_torus_config *c)
+{
+    // FixedBGTorusConfig defaults, FixedBGTorus.hpp:20-34
+    c->total_mass = 1.0;
+    c->inner_radius = 0.0;
+    c->pressure_max_radius = 0.0;
+    c->rho_peak = 1.0;
+    c->max_velocity_squared = 1.0 - 1.0e-12;
+    c->radial_derivative_fraction = 1.0e-3;
+    c->radial_derivative_min_step = 1.0e-4;
+    c->angular_momentum_min_factor = 0.25;
+    c->angular_momentum_max_factor = 4.0;
+    c->angular_momentum_samples = 120;
+    c->angular_momentum_bisection_iterations = 80;
+    c->angular_momentum_tolerance = 1.0e-13;
+}
+
+int grhd_torus_initial_data(grhd_ctx *ctx, double *state, int64_t state_cs,
+                            const grhd_box *box,
+                            const grhd_torus_config *config, double time,
+                            grhd_torus_params *out, void *stream)
+{
+    int st = common_checks(ctx, state, box);
+    if (st)
+        return st;
+    if (!config)
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "null torus config");
+    cudaStream_t s = (cudaStream_t)stream;
+    const BoxDev b = make_box(box, state_cs);
+    if ((st = check_strides(ctx, b, state_cs, -1)))
+        return st;
+    TorusConfigDev c;
+    static_assert(sizeof(TorusConfigDev) == sizeof(grhd_torus_config),
+                  "torus config layout");
+    std::memcpy(&c, config, sizeof(c));
+    const Background bg = make_background(ctx->params, time);
+    double res[4] = {0, 0, 0, 0};
+    ctx->launches += 3;
+    const cudaError_t e = torus_initial_data(state, b, bg, ctx->opt, c,
+                                             ctx->probe, res, s);
+    if (out)
+    {
+        out->ell = res[0];
+        out->surface_potential = res[1];
+        out->polytropic_constant = res[2];
+        out->max_enthalpy = res[3];
+    }
+    if (e == cudaErrorInvalidValue)
+        return set_error(ctx, GRHD_ERR_SETUP, 0, nullptr, 0.0,
+                         "torus has no pressure-supported region or an "
+                         "invalid surface potential");
+    GRHD_CUDA(ctx, e);
+    GRHD_CUDA(ctx, cudaStreamSynchronize(s));
+    return GRHD_OK;
+}
+
+int grhd_michel_initial_data(grhd_ctx *ctx, double *state, int64_t state_cs,
+                             const grhd_box *box,
+                             const grhd_michel_config *config, void *stream)
+{
+    int st = common_checks(ctx, state, box);
+    if (st)
+        return st;
+    if (!config)
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "null Michel config");
+    cudaStream_t s = (cudaStream_t)stream;
+    const BoxDev b = make_box(box, state_cs);
+    if ((st = check_strides(ctx, b, state_cs, -1)))
+        return st;
+    MichelConfigDev c;
+    c.mass = config->mass;
+    c.gamma = ctx->params.adiabatic_index;
+    c.sonic_radius = config->sonic_radius;
+    c.sonic_density = config->sonic_density;
+    c.atmosphere_radius = config->atmosphere_radius;
+    c.root_tolerance = config->root_tolerance;
+    ++ctx->launches;
+    GRHD_CUDA(ctx, michel_initial_data(state, b, ctx->opt, c, ctx->flag, s));
+    int bad = 0;
+    GRHD_CUDA(ctx, cudaMemcpyAsync(&bad, ctx->flag, sizeof(int),
+                                   cudaMemcpyDeviceToHost, s));
+    GRHD_CUDA(ctx, cudaStreamSynchronize(s));
+    if (bad)
+        return set_error(ctx, GRHD_ERR_SETUP, 0, nullptr, 0.0,
+                         "Michel profile has no root or an invalid Lorentz "
+                         "factor outside the atmosphere radius");
+    return GRHD_OK;
+}
+
+int grhd_perturb_density(grhd_ctx *ctx, double *state, int64_t state_cs,
+                         const grhd_box *box, double amplitude, uint64_t seed,
+                         double time, void *stream)
+{
+    int st = common_checks(ctx, state, box);
+    if (st)
+        return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    const BoxDev b = make_box(box, state_cs);
+    if ((st = check_strides(ctx, b, state_cs, -1)))
+        return st;
+    const Background bg = make_background(ctx->params, time);
+    ++ctx->launches;
+    GRHD_CUDA(ctx, perturb_density(state, b, bg, ctx->opt, amplitude, seed, s));
+    GRHD_CUDA(ctx, cudaStreamSynchronize(s));
+    return GRHD_OK;
+}
+
+int grhd_profile_enable(grhd_ctx *ctx, int enable)
+{
+    if (!ctx)
+        return GRHD_ERR_INVALID_ARG;
+    ctx->prof_on = enable != 0;
+    return GRHD_OK;
+}
+
+int grhd_profile_read(grhd_ctx *ctx, double ms[GRHD_K_NUM_CLASSES],
+                      long long launches[GRHD_K_NUM_CLASSES])
+{
+    if (!ctx || !ms || !launches)
+        return GRHD_ERR_INVALID_ARG;
+    for (int q = 0; q < GRHD_K_NUM_CLASSES; ++q)
+    {
+        ms[q] = 0.0;
+        launches[q] = 0;
+    }
+    for (auto &r : ctx->prof_pending)
+    {
+        GRHD_CUDA(ctx, cudaEventSynchronize(r.b));
+        float t = 0.0f;
+        GRHD_CUDA(ctx, cudaEventElapsedTime(&t, r.a, r.b));
+        if (r.cls >= 0 && r.cls < GRHD_K_NUM_CLASSES)
+        {
+            ms[r.cls] += t;
+            launches[r.cls] += 1;
+        }
+        ctx->event_pool.push_back(r.a);
+        ctx->event_pool.push_back(r.b);
+    }
+    ctx->prof_pending.clear();
+    return GRHD_OK;
+}
+
+long long grhd_launch_count(const grhd_ctx *ctx)
+{
+    return ctx ? ctx->launches : 0;
+}
+
+} // extern "C"

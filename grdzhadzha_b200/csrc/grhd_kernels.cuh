@@ -1,0 +1,116 @@
+// grhd_kernels.cuh -- kernels of the fixed-background GRHD operator and the
+// small host-side descriptors they take.
+#pragma once
+
+#include "grhd_device.cuh"
+
+namespace grhd {
+
+// One box of the level on the device: interior [lo,hi], ghosted storage
+// [glo,ghi], non-periodic domain [dlo,dhi]; cs / rcs are the component
+// strides of the state (11 components over the ghosted box) and of
+// interior-box arrays (5 components).
+struct BoxDev
+{
+    int lo[3], hi[3], glo[3], ghi[3], dlo[3], dhi[3];
+    int gn[3], in[3];
+    int64_t cs;  // state component stride
+    int64_t rcs; // interior array component stride
+    int64_t pcs; // primitive scratch component stride (ghosted volume)
+
+    __host__ __device__ int64_t gidx(int i, int j, int k) const
+    {
+        return (int64_t)(i - glo[0]) +
+               (int64_t)gn[0] * ((int64_t)(j - glo[1]) +
+                                 (int64_t)gn[1] * (int64_t)(k - glo[2]));
+    }
+    __host__ __device__ int64_t iidx(int i, int j, int k) const
+    {
+        return (int64_t)(i - lo[0]) +
+               (int64_t)in[0] * ((int64_t)(j - lo[1]) +
+                                 (int64_t)in[1] * (int64_t)(k - lo[2]));
+    }
+    __host__ __device__ int64_t gvol() const
+    {
+        return (int64_t)gn[0] * gn[1] * gn[2];
+    }
+    __host__ __device__ int64_t ivol() const
+    {
+        return (int64_t)in[0] * in[1] * in[2];
+    }
+};
+
+// Device-side status of one call: the first recovery failure in the
+// reference's iteration order (key = where << 56 | linear index), the
+// atmosphere-reset counters, and the CFL maximum (bit pattern of a
+// non-negative double, so integer max == floating max).
+struct DevStatus
+{
+    unsigned long long err_key;
+    unsigned long long counts[4];
+    unsigned long long maxinv_bits;
+};
+
+enum : int
+{
+    kStateComps = 11,
+    kD = 0,
+    kS1 = 1,
+    kTau = 4,
+    kRho = 5,
+    kEps = 6,
+    kPress = 7,
+    kV1 = 8
+};
+
+// Face kernel tiling: 16x16 threads own a 15x15 cell tile in (x, y) and
+// march along z.
+constexpr int kTB = 16;
+constexpr int kTC = 15;
+constexpr int kPW = kTC + 4; // primitive tile width (2 halo each side)
+constexpr int kGW = kTC + 2; // geometry tile width (1 halo each side)
+constexpr int kGeoFields = 16;
+
+size_t face_kernel_smem_bytes();
+// Per-device kernel attributes (dynamic shared memory of the face kernel).
+cudaError_t configure_kernels();
+
+void launch_fill_ghosts(double *state, const BoxDev &b, const Background &bg,
+                        const Options &o, DevStatus *st, cudaStream_t s);
+void launch_cells(const double *state, double *prim, double *src,
+                  const BoxDev &b, const Background &bg, const Options &o,
+                  DevStatus *st, cudaStream_t s);
+void launch_faces(const double *prim, const double *src, double *rhs,
+                  const BoxDev &b, const Background &bg, const Options &o,
+                  const double inv_dx[3], int zchunk, cudaStream_t s);
+// Strides: dcs / scs / ucs / ocs / tcs are the component strides of the
+// state-layout arrays each launcher names (11 components over the ghosted
+// box, indexed by BoxDev::gidx); b.rcs is the stride of rhs / k / acc.
+void launch_update(double *dst, int64_t dcs, const double *src_state,
+                   int64_t scs, const double *rhs, const BoxDev &b,
+                   const Background &bg, const Options &o, double dt,
+                   int recover, DevStatus *st, cudaStream_t s);
+void launch_recover(double *state, const BoxDev &b, const Background &bg,
+                    const Options &o, DevStatus *st, cudaStream_t s);
+void launch_ssprk2_combine(double *state, int64_t scs, const double *stage,
+                           int64_t tcs, const double *rhs, const BoxDev &b,
+                           const Background &bg, const Options &o, double dt,
+                           DevStatus *st, cudaStream_t s);
+void launch_rk4_stage(const double *un, int64_t ucs, double *out,
+                      int64_t ocs, const double *k, double *acc,
+                      const BoxDev &b, const Background &bg, const Options &o,
+                      int stage, double dt, DevStatus *st, cudaStream_t s);
+void launch_max_inv_dt(const double *state, const BoxDev &b,
+                       const Background &bg, const Options &o,
+                       const double inv_dx[3], DevStatus *st, cudaStream_t s);
+void launch_residual_probe(const double *state, const BoxDev &b,
+                           const Background &bg, const Options &o, int i,
+                           int j, int k, double *out, cudaStream_t s);
+void launch_eval_background(int64_t n, const double *xyz,
+                            const Background &bg, double *out,
+                            cudaStream_t s);
+void launch_eval_con2prim(int64_t n, const double *cons, const double *gUU,
+                          const Options &o, double *prim, int *ok, int *iters,
+                          double *resid, cudaStream_t s);
+
+} // namespace grhd

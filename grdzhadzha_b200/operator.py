@@ -1,0 +1,422 @@
+"""Python mirror of the reference operator classes over the C ABI.
+
+Names, arguments and error behaviour follow GRDzhadzha's
+Source/Matter/GRHD/FixedBGFArrayBoxFiniteVolume.hpp:
+
+  FixedBGLevelDataFiniteVolumeOperator(eos, background, dx, center,
+      atmosphere, limiter_theta, use_reconstruction, recovery_options,
+      use_static_metric_sources)                                   :446-614
+  TimeDependentFixedBGLevelDataFiniteVolumeOperator(eos, background_factory,
+      dx, center, atmosphere, limiter_theta, use_reconstruction,
+      recovery_options, use_static_metric_sources,
+      use_metric_volume_time_sources, metric_time_derivative_step)  :677-830
+
+A level here is one box (`LevelBox`) holding a CUDA float64 tensor of shape
+(11, nz + 2g, ny + 2g, nx + 2g) in the FArrayBox component order
+D, S1, S2, S3, tau, rho, eps, pressure, v1, v2, v3.  torch only supplies the
+device memory and the stream; all arithmetic runs in libgrhd_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import torch
+
+from . import _lib as L
+
+D, S1, S2, S3, TAU, RHO, EPS, PRESSURE, V1, V2, V3 = range(11)
+
+
+# ---------------------------------------------------------------- options
+
+
+@dataclass
+class IdealGasEOS:
+    """IdealGasEOS.hpp:10-53"""
+    adiabatic_index: float = 5.0 / 3.0
+
+
+@dataclass
+class AtmosphereOptions:
+    """Atmosphere.hpp:16-22"""
+    rho_floor: float = 1.0e-12
+    pressure_floor: float = 1.0e-12
+    max_velocity_squared: float = 1.0 - 1.0e-12
+    metric_source_atmosphere_factor: float = 1.0 + 1.0e-12
+
+
+@dataclass
+class RecoveryOptions:
+    """Valencia.hpp:17-23"""
+    max_iterations: int = 50
+    tolerance: float = 1.0e-12
+    pressure_floor: float = 1.0e-12
+    max_velocity_squared: float = 1.0 - 1.0e-12
+
+
+@dataclass
+class KerrSchild:
+    """KerrSchild.hpp:22-90 (params_t + dx).  The hole sits at the
+    operator centre; `center` is kept for interface parity."""
+    mass: float = 1.0
+    spin: float = 0.0
+    center: Sequence[float] = (0.0, 0.0, 0.0)
+    dx: float = 1.0
+
+    def __post_init__(self):
+        if self.spin > self.mass or self.spin < -self.mass:
+            raise ValueError("The dimensionless spin parameter must be in the "
+                             "range -1.0 < spin < 1.0")
+
+
+@dataclass
+class CircularBinaryPN:
+    """CircularBinaryPN.hpp:29-57 (params_t + dx).  Used directly as the
+    time-dependent operator's background factory: factory(t) is this
+    binary with params.time + t (Tests/GRHDFixedBGTest/GRHDFixedBGTest.cpp:
+    435-446)."""
+    mass_1: float = 0.5
+    mass_2: float = 0.5
+    separation: float = 10.0
+    angular_velocity: float = 0.0
+    phase: float = 0.0
+    time: float = 0.0
+    softening_radius: float = 0.5
+    center: Sequence[float] = (0.0, 0.0, 0.0)
+    dx: float = 1.0
+
+    def __post_init__(self):
+        if (self.mass_1 <= 0.0 or self.mass_2 <= 0.0 or self.separation <= 0.0
+                or self.softening_radius < 0.0):
+            raise ValueError("Invalid CircularBinaryPN parameters")
+
+
+# ------------------------------------------------------------------ level
+
+
+@dataclass
+class LevelBox:
+    """One box of a level: interior [lo, hi], ghost width, problem domain
+    and the device state tensor over the ghosted box."""
+    lo: tuple
+    hi: tuple
+    ghost: int = 2
+    domain_lo: tuple | None = None
+    domain_hi: tuple | None = None
+    state: torch.Tensor | None = field(default=None, repr=False)
+    device: str = "cuda"
+
+    def __post_init__(self):
+        if self.domain_lo is None:
+            self.domain_lo = tuple(self.lo)
+        if self.domain_hi is None:
+            self.domain_hi = tuple(self.hi)
+        if self.state is None:
+            g = self.ghost
+            n = [self.hi[d] - self.lo[d] + 1 + 2 * g for d in range(3)]
+            self.state = torch.zeros((11, n[2], n[1], n[0]),
+                                     dtype=torch.float64, device=self.device)
+
+    @classmethod
+    def cube(cls, n, ghost=2, device="cuda"):
+        nn = (n, n, n) if isinstance(n, int) else tuple(n)
+        return cls(lo=(0, 0, 0), hi=tuple(x - 1 for x in nn), ghost=ghost,
+                   device=device)
+
+    @property
+    def interior_shape(self):
+        return tuple(self.hi[d] - self.lo[d] + 1 for d in (2, 1, 0))
+
+    @property
+    def num_cells(self) -> int:
+        s = self.interior_shape
+        return s[0] * s[1] * s[2]
+
+    def interior(self, comps=slice(0, 11)) -> torch.Tensor:
+        g = self.ghost
+        z, y, x = self.interior_shape
+        return self.state[comps, g:g + z, g:g + y, g:g + x]
+
+    def c_box(self) -> L.Box:
+        b = L.Box()
+        for d in range(3):
+            b.lo[d], b.hi[d] = self.lo[d], self.hi[d]
+            b.domain_lo[d], b.domain_hi[d] = self.domain_lo[d], self.domain_hi[d]
+        b.ghost = self.ghost
+        return b
+
+    def comp_stride(self) -> int:
+        return self.state[0].numel()
+
+    def new_rhs(self) -> torch.Tensor:
+        return torch.zeros((5,) + self.interior_shape, dtype=torch.float64,
+                           device=self.state.device)
+
+
+def _ptr(t: torch.Tensor):
+    if not t.is_cuda or t.dtype != torch.float64 or not t.is_contiguous():
+        raise ValueError("expected a contiguous CUDA float64 tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+# --------------------------------------------------------------- operators
+
+
+class _OperatorBase:
+    def __init__(self, eos, background, dx, center, atmosphere,
+                 limiter_theta, use_reconstruction, recovery_options,
+                 use_static_metric_sources, use_metric_volume_time_sources,
+                 metric_time_derivative_step, excision_radius):
+        if not dx > 0.0:
+            raise ValueError("GRHD grid spacing must be positive")
+        self._lib = L.load()
+        p = L.Params()
+        self._lib.grhd_default_params(C.byref(p))
+        if isinstance(background, KerrSchild):
+            p.background = L.GRHD_BG_KERR_SCHILD
+            p.ks_mass, p.ks_spin = background.mass, background.spin
+        elif isinstance(background, CircularBinaryPN):
+            p.background = L.GRHD_BG_BINARY_PN
+            p.pn_mass_1, p.pn_mass_2 = background.mass_1, background.mass_2
+            p.pn_separation = background.separation
+            p.pn_angular_velocity = background.angular_velocity
+            p.pn_phase, p.pn_time = background.phase, background.time
+            p.pn_softening_radius = background.softening_radius
+        else:
+            raise TypeError("background must be KerrSchild or CircularBinaryPN")
+        p.adiabatic_index = eos.adiabatic_index
+        p.dx = dx
+        for d in range(3):
+            p.center[d] = center[d]
+        a = atmosphere or AtmosphereOptions()
+        p.rho_floor, p.pressure_floor = a.rho_floor, a.pressure_floor
+        p.max_velocity_squared = a.max_velocity_squared
+        p.metric_source_atmosphere_factor = a.metric_source_atmosphere_factor
+        r = recovery_options or RecoveryOptions()
+        p.recovery_max_iterations = r.max_iterations
+        p.recovery_tolerance = r.tolerance
+        p.recovery_pressure_floor = r.pressure_floor
+        p.recovery_max_velocity_squared = r.max_velocity_squared
+        p.limiter_theta = limiter_theta
+        p.use_reconstruction = int(use_reconstruction)
+        p.use_static_metric_sources = int(use_static_metric_sources)
+        p.use_metric_volume_time_sources = int(use_metric_volume_time_sources)
+        p.metric_time_derivative_step = metric_time_derivative_step
+        p.excision_radius = excision_radius
+        self.params = p
+        self.dx = dx
+        self.eos = eos
+        self.background = background
+        ctx = C.c_void_p()
+        L.check(self._lib, None, self._lib.grhd_create(C.byref(p),
+                                                       C.byref(ctx)))
+        self._ctx = ctx
+
+    def __del__(self):
+        ctx = getattr(self, "_ctx", None)
+        if ctx:
+            self._lib.grhd_destroy(ctx)
+            self._ctx = None
+
+    def _inv(self, inverse_dx_U):
+        v = inverse_dx_U if inverse_dx_U is not None else [1.0 / self.dx] * 3
+        return (C.c_double * 3)(*v)
+
+    def _check(self, status):
+        L.check(self._lib, self._ctx, status)
+
+    # ---- methods of the reference operator ----
+
+    def _compute_rhs(self, rhs, state: LevelBox, inverse_dx_U, time):
+        b = state.c_box()
+        self._check(self._lib.grhd_compute_rhs(
+            self._ctx, _ptr(rhs), rhs[0].numel(), _ptr(state.state),
+            state.comp_stride(), C.byref(b), self._inv(inverse_dx_U), time,
+            _stream()))
+
+    def _recover_primitives(self, state: LevelBox, time):
+        d = L.Diagnostics()
+        b = state.c_box()
+        self._check(self._lib.grhd_recover_primitives(
+            self._ctx, _ptr(state.state), state.comp_stride(), C.byref(b),
+            time, C.byref(d), _stream()))
+        return d
+
+    def _update_conserved(self, state, rhs, dt, recovery_time, recover):
+        d = L.Diagnostics()
+        b = state.c_box()
+        self._check(self._lib.grhd_update_conserved(
+            self._ctx, _ptr(state.state), state.comp_stride(), _ptr(rhs),
+            rhs[0].numel(), C.byref(b), dt, recovery_time, int(recover),
+            C.byref(d), _stream()))
+        return d
+
+    def _compute_max_inverse_dt(self, state, inverse_dx_U, time):
+        out = C.c_double()
+        b = state.c_box()
+        self._check(self._lib.grhd_compute_max_inverse_dt(
+            self._ctx, _ptr(state.state), state.comp_stride(), C.byref(b),
+            self._inv(inverse_dx_U), time, C.byref(out), _stream()))
+        return out.value
+
+    def _compute_stable_dt(self, state, inverse_dx_U, cfl, time):
+        if not cfl > 0.0:
+            raise L.InvalidArgument(L.GRHD_ERR_INVALID_ARG, None)
+        out = C.c_double()
+        b = state.c_box()
+        self._check(self._lib.grhd_compute_stable_dt(
+            self._ctx, _ptr(state.state), state.comp_stride(), C.byref(b),
+            self._inv(inverse_dx_U), cfl, time, C.byref(out), _stream()))
+        return out.value
+
+    def _advance(self, fn, state, inverse_dx_U, time, dt):
+        d = L.Diagnostics()
+        b = state.c_box()
+        self._check(fn(self._ctx, _ptr(state.state), state.comp_stride(),
+                       C.byref(b), self._inv(inverse_dx_U), time, dt,
+                       C.byref(d), _stream()))
+        return d
+
+    # ---- initial data (FixedBGTorus.hpp, Michel test) ----
+
+    def fill_torus(self, state: LevelBox, inner_radius, pressure_max_radius,
+                   rho_peak=1.0, total_mass=1.0, max_velocity_squared=None,
+                   time=0.0):
+        """make_fixed_bg_torus_parameters + fill_fixed_bg_torus_level_data
+        (FixedBGTorus.hpp:291-409) on the device; returns the torus
+        parameters (ell, surface_potential, polytropic_constant,
+        max_enthalpy)."""
+        c = L.TorusConfig()
+        self._lib.grhd_default_torus_config(C.byref(c))
+        c.total_mass, c.inner_radius = total_mass, inner_radius
+        c.pressure_max_radius, c.rho_peak = pressure_max_radius, rho_peak
+        if max_velocity_squared is not None:
+            c.max_velocity_squared = max_velocity_squared
+        out = L.TorusParams()
+        b = state.c_box()
+        self._check(self._lib.grhd_torus_initial_data(
+            self._ctx, _ptr(state.state), state.comp_stride(), C.byref(b),
+            C.byref(c), time, C.byref(out), _stream()))
+        return out
+
+    def fill_michel(self, state: LevelBox, sonic_radius=8.0,
+                    sonic_density=1.0e-6, atmosphere_radius=4.0,
+                    mass=1.0, root_tolerance=1.0e-13):
+        """fill_michel_state (Tests/GRHDLevelDataMichelAccretion:312-372)."""
+        c = L.MichelConfig(mass, sonic_radius, sonic_density,
+                           atmosphere_radius, root_tolerance)
+        b = state.c_box()
+        self._check(self._lib.grhd_michel_initial_data(
+            self._ctx, _ptr(state.state), state.comp_stride(), C.byref(b),
+            C.byref(c), _stream()))
+
+    def perturb_density(self, state: LevelBox, amplitude, seed, time=0.0):
+        b = state.c_box()
+        self._check(self._lib.grhd_perturb_density(
+            self._ctx, _ptr(state.state), state.comp_stride(), C.byref(b),
+            amplitude, seed, time, _stream()))
+
+    # ---- instrumentation ----
+
+    def profile(self, enable=True):
+        self._check(self._lib.grhd_profile_enable(self._ctx, int(enable)))
+
+    def profile_read(self):
+        """{class: (ms, launches)} since the last read."""
+        ms = (C.c_double * L.NUM_KERNEL_CLASSES)()
+        n = (C.c_longlong * L.NUM_KERNEL_CLASSES)()
+        self._check(self._lib.grhd_profile_read(self._ctx, ms, n))
+        return {name: (ms[i], n[i])
+                for i, name in enumerate(L.KERNEL_CLASSES)}
+
+    def launch_count(self) -> int:
+        return int(self._lib.grhd_launch_count(self._ctx))
+
+    def advance_rk4(self, state, inverse_dx_U=None, time=0.0, dt=None):
+        """New: classic RK4 with post-stage recovery (no reference
+        counterpart)."""
+        return self._advance(self._lib.grhd_advance_rk4, state, inverse_dx_U,
+                             time, dt)
+
+
+class FixedBGLevelDataFiniteVolumeOperator(_OperatorBase):
+    """FixedBGFArrayBoxFiniteVolume.hpp:446-614 (static background)."""
+
+    def __init__(self, eos, background, dx, center,
+                 atmosphere=None, limiter_theta=1.5, use_reconstruction=True,
+                 recovery_options=None, use_static_metric_sources=True,
+                 excision_radius=0.0):
+        super().__init__(eos, background, dx, center, atmosphere,
+                         limiter_theta, use_reconstruction, recovery_options,
+                         use_static_metric_sources, False, 1.0e-3,
+                         excision_radius)
+
+    def compute_rhs(self, rhs, state, domain=None, inverse_dx_U=None):
+        self._compute_rhs(rhs, state, inverse_dx_U, 0.0)
+
+    def recover_primitives(self, state):
+        return self._recover_primitives(state, 0.0)
+
+    def update_conserved(self, state, rhs, dt,
+                         recover_primitives_after_update=True):
+        return self._update_conserved(state, rhs, dt, 0.0,
+                                      recover_primitives_after_update)
+
+    def compute_max_inverse_dt(self, state, domain_box=None,
+                               inverse_dx_U=None):
+        return self._compute_max_inverse_dt(state, inverse_dx_U, 0.0)
+
+    def compute_stable_dt(self, state, domain_box=None, inverse_dx_U=None,
+                          cfl=None):
+        return self._compute_stable_dt(state, inverse_dx_U, cfl, 0.0)
+
+    def advance_ssprk2(self, state, domain=None, inverse_dx_U=None, dt=None):
+        return self._advance(self._lib.grhd_advance_ssprk2, state,
+                             inverse_dx_U, 0.0, dt)
+
+
+class TimeDependentFixedBGLevelDataFiniteVolumeOperator(_OperatorBase):
+    """FixedBGFArrayBoxFiniteVolume.hpp:677-830 (background factory of
+    time; the CircularBinaryPN parameters act as the factory)."""
+
+    def __init__(self, eos, background_factory, dx, center,
+                 atmosphere=None, limiter_theta=1.5, use_reconstruction=True,
+                 recovery_options=None, use_static_metric_sources=True,
+                 use_metric_volume_time_sources=True,
+                 metric_time_derivative_step=1.0e-3, excision_radius=0.0):
+        super().__init__(eos, background_factory, dx, center, atmosphere,
+                         limiter_theta, use_reconstruction, recovery_options,
+                         use_static_metric_sources,
+                         use_metric_volume_time_sources,
+                         metric_time_derivative_step, excision_radius)
+
+    def compute_rhs(self, rhs, state, domain=None, inverse_dx_U=None,
+                    time=0.0):
+        self._compute_rhs(rhs, state, inverse_dx_U, time)
+
+    def recover_primitives(self, state, time=0.0):
+        return self._recover_primitives(state, time)
+
+    def update_conserved(self, state, rhs, dt, recovery_time=0.0,
+                         recover_primitives_after_update=True):
+        return self._update_conserved(state, rhs, dt, recovery_time,
+                                      recover_primitives_after_update)
+
+    def compute_max_inverse_dt(self, state, domain_box=None,
+                               inverse_dx_U=None, time=0.0):
+        return self._compute_max_inverse_dt(state, inverse_dx_U, time)
+
+    def compute_stable_dt(self, state, domain_box=None, inverse_dx_U=None,
+                          cfl=None, time=0.0):
+        return self._compute_stable_dt(state, inverse_dx_U, cfl, time)
+
+    def advance_ssprk2(self, state, domain=None, inverse_dx_U=None, time=0.0,
+                       dt=None):
+        return self._advance(self._lib.grhd_advance_ssprk2, state,
+                             inverse_dx_U, time, dt)

@@ -1,0 +1,301 @@
+/*
+ * grhd_b200.h -- C ABI of the B200 (sm_100a) fixed-background Valencia GRHD
+ * operator.
+ *
+ * The entry points replace the methods of the reference's operator classes
+ * (GRDzhadzha Source/Matter/GRHD/FixedBGFArrayBoxFiniteVolume.hpp):
+ *
+ *   FixedBGLevelDataFiniteVolumeOperator<eos_t, background_t>       :446-614
+ *   TimeDependentFixedBGLevelDataFiniteVolumeOperator<eos_t, fac_t> :677-830
+ *
+ * One call works on one box of a level (one Chombo FArrayBox): the caller
+ * owns every array; the library holds only parameters and its own scratch.
+ *
+ * Storage (the FArrayBox layout of the reference, Chombo Fortran order):
+ *   the state array covers the ghosted box  glo = lo - ghost, ghi = hi + ghost,
+ *   value(i,j,k,c) = state[c * state_comp_stride
+ *                          + (i-glo0) + nx*((j-glo1) + ny*(k-glo2))]
+ *   nx = ghi0-glo0+1, ny = ghi1-glo1+1, state_comp_stride >= nx*ny*nz,
+ *   components in the order of the reference UserVariables
+ *   (Tests/GRHDFixedBGTest/UserVariables.hpp:24-40) counted from c_GRHD_D:
+ *     0 D, 1 S1, 2 S2, 3 S3, 4 tau, 5 rho, 6 eps, 7 pressure, 8 v1, 9 v2, 10 v3
+ *   so a caller holding a full GRChombo FAB passes &fab(lo, c_GRHD_D).
+ * Right-hand sides cover the interior box only (the reference's rhs
+ * LevelData has zero ghosts): 5 components D, S1, S2, S3, tau.
+ *
+ * All pointers are device pointers (cudaMalloc'd or managed).  `stream` is a
+ * cudaStream_t passed as void* (NULL = legacy default stream).  Every call is
+ * ordered on that stream; calls that return host values (diagnostics, dt,
+ * status) synchronise the stream before returning.  A context may be used by
+ * one thread at a time; distinct contexts are independent.
+ *
+ * Error behaviour mirrors the reference's exceptions: a con2prim failure on
+ * an RHS, boundary or CFL path (the reference throws std::runtime_error,
+ * :48-55, :157-164, :272-279, :383-390) returns GRHD_ERR_RECOVERY and
+ * grhd_last_error() gives the failing cell and residual; cfl <= 0 or dx <= 0
+ * (std::invalid_argument, :549-550, FixedBGLevelDataDriver.hpp:36-38)
+ * returns GRHD_ERR_INVALID_ARG.  After an error the state is unspecified.
+ */
+#ifndef GRHD_B200_H_
+#define GRHD_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GRHD_B200_ABI_VERSION 1
+
+typedef struct grhd_ctx grhd_ctx;
+
+typedef enum grhd_status
+{
+    GRHD_OK = 0,
+    GRHD_ERR_RECOVERY = 1,    /* con2prim failed where the reference throws */
+    GRHD_ERR_INVALID_ARG = 2, /* bad argument (cfl, dx, box, pointer)       */
+    GRHD_ERR_CUDA = 3,        /* CUDA runtime error                          */
+    GRHD_ERR_SETUP = 4        /* initial data could not be constructed       */
+} grhd_status;
+
+typedef enum grhd_background_kind
+{
+    GRHD_BG_KERR_SCHILD = 0, /* Source/Background/KerrSchild.hpp        */
+    GRHD_BG_BINARY_PN = 1    /* Source/Background/CircularBinaryPN.hpp  */
+} grhd_background_kind;
+
+/* Where a recovery failure happened (the reference's message variants). */
+typedef enum grhd_error_where
+{
+    GRHD_WHERE_NONE = 0,
+    GRHD_WHERE_OUTFLOW_SOURCE = 1,    /* boundary fill,  :157-164 */
+    GRHD_WHERE_GHOSTED_RECOVERY = 2,  /* ghosted box,    :48-55   */
+    GRHD_WHERE_METRIC_SOURCES = 3,    /* sources,        :272-279 */
+    GRHD_WHERE_CFL = 4                /* CFL speed,      :383-390 */
+} grhd_error_where;
+
+/* Operator parameters: the constructor arguments of the reference operators
+ * (:450-464 and :681-700) with the EOS (IdealGasEOS.hpp:13-16), background
+ * params_t (KerrSchild.hpp:26-31, CircularBinaryPN.hpp:32-42),
+ * AtmosphereOptions (Atmosphere.hpp:16-22) and RecoveryOptions
+ * (Valencia.hpp:17-23) flattened in.  grhd_default_params() fills the
+ * reference defaults.  Fields marked "new" have no reference counterpart. */
+typedef struct grhd_params
+{
+    int background; /* grhd_background_kind */
+    double ks_mass, ks_spin;
+    double pn_mass_1, pn_mass_2, pn_separation, pn_angular_velocity,
+        pn_phase, pn_time, pn_softening_radius;
+    double adiabatic_index;
+    double dx;
+    double center[3];
+    double rho_floor, pressure_floor, max_velocity_squared,
+        metric_source_atmosphere_factor;
+    int recovery_max_iterations;
+    double recovery_tolerance, recovery_pressure_floor,
+        recovery_max_velocity_squared;
+    double limiter_theta;
+    int use_reconstruction, use_static_metric_sources,
+        use_metric_volume_time_sources;
+    double metric_time_derivative_step;
+    double excision_radius; /* new: cells with coordinate radius below this
+                               are frozen and get a zero RHS; <= 0 disables */
+} grhd_params;
+
+/* One box of the level.  lo/hi: the box's valid cells (inclusive); ghost:
+ * ghost width of its storage (>= 2); domain_lo/hi: the non-periodic
+ * problem domain.  Ghost cells outside the domain are physical boundaries
+ * (outflow); ghost cells inside it are the caller's (exchange). */
+typedef struct grhd_box
+{
+    int lo[3], hi[3];
+    int ghost;
+    int domain_lo[3], domain_hi[3];
+} grhd_box;
+
+/* AtmosphereResetDiagnostics, FArrayBoxFiniteVolume.hpp:78-92 */
+typedef struct grhd_diagnostics
+{
+    long long num_cells, num_failed_recoveries, num_floored_primitives,
+        num_conserved_resets;
+} grhd_diagnostics;
+
+typedef struct grhd_error
+{
+    int status;    /* grhd_status of the failing call */
+    int where;     /* grhd_error_where */
+    int cell[3];   /* failing cell (level index space) */
+    double residual;
+    char message[256];
+} grhd_error;
+
+/* ---- context ---- */
+void grhd_default_params(grhd_params *params);
+/* Creates a context for `params` on the current CUDA device.  Replaces the
+ * operator constructor (:450-464 / :681-700). */
+int grhd_create(const grhd_params *params, grhd_ctx **out);
+void grhd_destroy(grhd_ctx *ctx);
+int grhd_last_error(const grhd_ctx *ctx, grhd_error *out);
+const char *grhd_status_string(int status);
+int grhd_abi_version(void);
+
+/* ---- operator methods ---- */
+
+/* compute_rhs(rhs, state, domain, inverse_dx_U[, time]), :468-477 / :702-720.
+ * Fills the physical ghosts of `state` (conserved and primitive components),
+ * then writes the flux-divergence + static-metric (+ volume-time) RHS over
+ * the interior.  `time` is ignored by the static Kerr-Schild background. */
+int grhd_compute_rhs(grhd_ctx *ctx, double *rhs, int64_t rhs_comp_stride,
+                     double *state, int64_t state_comp_stride,
+                     const grhd_box *box, const double inverse_dx[3],
+                     double time, void *stream);
+
+/* recover_primitives(state[, time]) -> AtmosphereResetDiagnostics,
+ * :506-520 / :728-743.  `diag` may be NULL. */
+int grhd_recover_primitives(grhd_ctx *ctx, double *state,
+                            int64_t state_comp_stride, const grhd_box *box,
+                            double time, grhd_diagnostics *diag, void *stream);
+
+/* update_conserved(state, rhs, dt[, recovery_time], recover), :522-533 /
+ * :745-757.  `diag` may be NULL. */
+int grhd_update_conserved(grhd_ctx *ctx, double *state,
+                          int64_t state_comp_stride, const double *rhs,
+                          int64_t rhs_comp_stride, const grhd_box *box,
+                          double dt, double recovery_time, int recover,
+                          grhd_diagnostics *diag, void *stream);
+
+/* compute_max_inverse_dt(state, domain_box, inverse_dx_U[, time]),
+ * :535-542 / :759-767. */
+int grhd_compute_max_inverse_dt(grhd_ctx *ctx, const double *state,
+                                int64_t state_comp_stride,
+                                const grhd_box *box,
+                                const double inverse_dx[3], double time,
+                                double *out, void *stream);
+
+/* compute_stable_dt(state, domain_box, inverse_dx_U, cfl[, time]),
+ * :544-555 / :769-780. */
+int grhd_compute_stable_dt(grhd_ctx *ctx, const double *state,
+                           int64_t state_comp_stride, const grhd_box *box,
+                           const double inverse_dx[3], double cfl,
+                           double time, double *out, void *stream);
+
+/* advance_ssprk2(state, domain, inverse_dx_U, [time,] dt), :563-589 /
+ * :782-809.  `diag` (may be NULL) accumulates the recovery counts of both
+ * post-update recoveries. */
+int grhd_advance_ssprk2(grhd_ctx *ctx, double *state,
+                        int64_t state_comp_stride, const grhd_box *box,
+                        const double inverse_dx[3], double time, double dt,
+                        grhd_diagnostics *diag, void *stream);
+
+/* New (no reference counterpart; the reference integrates with SSPRK2
+ * only): classic four-stage RK4 with the reference's post-update recovery
+ * after every stage, stage times t, t+dt/2, t+dt/2, t+dt. */
+int grhd_advance_rk4(grhd_ctx *ctx, double *state, int64_t state_comp_stride,
+                     const grhd_box *box, const double inverse_dx[3],
+                     double time, double dt, grhd_diagnostics *diag,
+                     void *stream);
+
+/* ---- pointwise kernels for verification ---- */
+
+/* ADM background vars at n points (xyz[3n], positions relative to the
+ * operator centre) at operator time `time`, laid out per point as
+ * gamma[9], K_tensor[9], K, lapse, shift[3], d1_gamma[27] ([i][j][k] =
+ * d_k gamma_ij), d1_lapse[3], d1_shift[9] ([i][j] = d_j shift^i): 64
+ * doubles.  Same quantities as KerrSchild/CircularBinaryPN::
+ * compute_metric_background (KerrSchild.hpp:64-166,
+ * CircularBinaryPN.hpp:70-189).  Device pointers. */
+int grhd_eval_background(grhd_ctx *ctx, int64_t n, const double *xyz,
+                         double time, double *out, void *stream);
+
+/* recover_primitive (Valencia.hpp:116-228) at n points: cons[5n] (D,S,tau),
+ * gUU[9n]; writes prim[6n] (rho,eps,p,v), ok[n], iterations[n],
+ * residual[n].  Device pointers. */
+int grhd_eval_con2prim(grhd_ctx *ctx, int64_t n, const double *cons,
+                       const double *gUU, double *prim, int *ok,
+                       int *iterations, double *residual, void *stream);
+
+/* ---- initial data (setup, not part of a step) ---- */
+
+/* FixedBGTorusConfig, Source/Matter/GRHD/FixedBGTorus.hpp:20-34 */
+typedef struct grhd_torus_config
+{
+    double total_mass, inner_radius, pressure_max_radius, rho_peak,
+        max_velocity_squared, radial_derivative_fraction,
+        radial_derivative_min_step, angular_momentum_min_factor,
+        angular_momentum_max_factor;
+    int angular_momentum_samples, angular_momentum_bisection_iterations;
+    double angular_momentum_tolerance;
+} grhd_torus_config;
+
+/* FixedBGTorusParameters, FixedBGTorus.hpp:36-42 */
+typedef struct grhd_torus_params
+{
+    double ell, surface_potential, polytropic_constant, max_enthalpy;
+} grhd_torus_params;
+
+void grhd_default_torus_config(grhd_torus_config *config);
+
+/* make_fixed_bg_torus_parameters + fill_fixed_bg_torus_level_data
+ * (FixedBGTorus.hpp:291-409) on the device: the angular-momentum solve, the
+ * maximum enthalpy over the box interior and the primitive + conserved fill
+ * of the whole ghosted box, with the operator's EOS, background (at `time`)
+ * and atmosphere.  `out` may be NULL.  Returns GRHD_ERR_SETUP when the
+ * torus has no pressure-supported region. */
+int grhd_torus_initial_data(grhd_ctx *ctx, double *state,
+                            int64_t state_comp_stride, const grhd_box *box,
+                            const grhd_torus_config *config, double time,
+                            grhd_torus_params *out, void *stream);
+
+/* MichelConfig of Tests/GRHDLevelDataMichelAccretion (:32-45); the EOS
+ * index is the operator's.  The operator's background must be the
+ * Kerr-Schild hole of the same mass with zero spin. */
+typedef struct grhd_michel_config
+{
+    double mass, sonic_radius, sonic_density, atmosphere_radius,
+        root_tolerance;
+} grhd_michel_config;
+
+/* fill_michel_state (GRHDLevelDataMichelAccretion.cpp:312-372) on the
+ * device: analytic Michel primitives outside atmosphere_radius (Bernoulli
+ * root solve per cell), atmosphere inside, floors, conserved variables. */
+int grhd_michel_initial_data(grhd_ctx *ctx, double *state,
+                             int64_t state_comp_stride, const grhd_box *box,
+                             const grhd_michel_config *config, void *stream);
+
+/* New: rho *= 1 + amplitude * u with u uniform in [-1, 1) from a
+ * counter-based hash of (seed, cell); pressure and velocity kept, eps and
+ * the conserved variables recomputed (whole ghosted box). */
+int grhd_perturb_density(grhd_ctx *ctx, double *state,
+                         int64_t state_comp_stride, const grhd_box *box,
+                         double amplitude, uint64_t seed, double time,
+                         void *stream);
+
+/* ---- instrumentation ---- */
+
+/* Kernel classes timed by the profiler. */
+typedef enum grhd_kernel_class
+{
+    GRHD_K_GHOSTS = 0, /* physical ghost fill                         */
+    GRHD_K_CELLS = 1,  /* per-cell con2prim + sources                 */
+    GRHD_K_FACES = 2,  /* face fluxes + divergence                    */
+    GRHD_K_STAGE = 3,  /* update / RK stage / recovery                */
+    GRHD_K_CFL = 4,    /* max inverse dt reduction                    */
+    GRHD_K_NUM_CLASSES = 5
+} grhd_kernel_class;
+
+/* Enables (1) or disables (0) CUDA-event timing of every kernel the
+ * context launches, on the stream it is launched on. */
+int grhd_profile_enable(grhd_ctx *ctx, int enable);
+/* Synchronises the recorded events and returns, per kernel class, the
+ * summed device time in ms and the number of launches since the last
+ * read; then clears them. */
+int grhd_profile_read(grhd_ctx *ctx, double ms[GRHD_K_NUM_CLASSES],
+                      long long launches[GRHD_K_NUM_CLASSES]);
+/* Total number of kernels this context has launched. */
+long long grhd_launch_count(const grhd_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRHD_B200_H_ */

@@ -1317,14 +1317,109 @@ int orc_compute_rhs_slabs(const orc_params *p, const orc_box *box,
     return status;
 }
 
+/* ------------------------------------------------------------------------ */
+/* z-parallel loops for the setup passes (initial data, recovery).  Cells   */
+/* are independent in these passes, so splitting k changes no result.      */
+/* ------------------------------------------------------------------------ */
+
+static int g_threads = 1;
+
+void orc_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
+
+typedef void (*zrange_fn)(void *ctx, int k0, int k1, int slot);
+
+typedef struct
+{
+    zrange_fn fn;
+    void *ctx;
+    int k0, k1, slot;
+} ZJob;
+
+static void *zjob_run(void *arg)
+{
+    ZJob *j = (ZJob *)arg;
+    j->fn(j->ctx, j->k0, j->k1, j->slot);
+    return NULL;
+}
+
+/* Runs fn over [klo, khi] split into at most g_threads contiguous chunks;
+ * returns the number of slots used. */
+static int parallel_z(int klo, int khi, zrange_fn fn, void *ctx, int max_slots)
+{
+    const int nz = khi - klo + 1;
+    int n = g_threads < max_slots ? g_threads : max_slots;
+    if (n > nz)
+        n = nz;
+    if (n <= 1)
+    {
+        fn(ctx, klo, khi, 0);
+        return 1;
+    }
+    ZJob jobs[256];
+    pthread_t th[256];
+    for (int s = 0; s < n; ++s)
+    {
+        jobs[s].fn = fn;
+        jobs[s].ctx = ctx;
+        jobs[s].k0 = klo + (nz * s) / n;
+        jobs[s].k1 = klo + (nz * (s + 1)) / n - 1;
+        jobs[s].slot = s;
+        pthread_create(&th[s], NULL, zjob_run, &jobs[s]);
+    }
+    for (int s = 0; s < n; ++s)
+        pthread_join(th[s], NULL);
+    return n;
+}
+
+static void recover_range(const orc_params *o, const orc_box *b,
+                          double *state, double t, int k0, int k1,
+                          orc_diag *out);
+
+typedef struct
+{
+    const orc_params *o;
+    const orc_box *b;
+    double *state;
+    double t;
+    orc_diag d[256];
+} RecoverCtx;
+
+static void recover_job(void *ctx, int k0, int k1, int slot)
+{
+    RecoverCtx *c = (RecoverCtx *)ctx;
+    recover_range(c->o, c->b, c->state, c->t, k0, k1, &c->d[slot]);
+}
+
 /* recover_primitives_and_apply_atmosphere_from_fixed_background,
  * FixedBGFArrayBoxFiniteVolume.hpp:60-110 */
 int orc_recover_primitives(const orc_params *o, const orc_box *b,
                            double *state, double t, orc_diag *diag)
 {
+    RecoverCtx *c = (RecoverCtx *)calloc(1, sizeof(RecoverCtx));
+    c->o = o;
+    c->b = b;
+    c->state = state;
+    c->t = t;
+    const int n = parallel_z(b->lo[2], b->hi[2], recover_job, c, 256);
+    if (diag)
+        for (int s = 0; s < n; ++s)
+        {
+            diag->num_cells += c->d[s].num_cells;
+            diag->num_failed_recoveries += c->d[s].num_failed_recoveries;
+            diag->num_floored_primitives += c->d[s].num_floored_primitives;
+            diag->num_conserved_resets += c->d[s].num_conserved_resets;
+        }
+    free(c);
+    return ORC_OK;
+}
+
+static void recover_range(const orc_params *o, const orc_box *b,
+                          double *state, double t, int k0, int k1,
+                          orc_diag *diag)
+{
     orc_diag dg;
     memset(&dg, 0, sizeof(dg));
-    for (int k = b->lo[2]; k <= b->hi[2]; ++k)
+    for (int k = k0; k <= k1; ++k)
         for (int j = b->lo[1]; j <= b->hi[1]; ++j)
             for (int i = b->lo[0]; i <= b->hi[0]; ++i)
             {
@@ -1362,14 +1457,7 @@ int orc_recover_primitives(const orc_params *o, const orc_box *b,
                     store_cons(b, state, idx, &nc);
                 }
             }
-    if (diag)
-    {
-        diag->num_cells += dg.num_cells;
-        diag->num_failed_recoveries += dg.num_failed_recoveries;
-        diag->num_floored_primitives += dg.num_floored_primitives;
-        diag->num_conserved_resets += dg.num_conserved_resets;
-    }
-    return ORC_OK;
+    *diag = dg;
 }
 
 /* compute_max_inverse_dt_from_fixed_background, :364-412 */
@@ -1915,6 +2003,49 @@ static double torus_enthalpy(double W, const orc_torus_params *t)
     return exp(t->surface_potential - W);
 }
 
+typedef struct
+{
+    const orc_params *p;
+    const orc_torus_config *c;
+    const orc_box *b;
+    double t;
+    const orc_torus_params *tp;
+    double hmax[256];
+} TorusMaxCtx;
+
+/* the maximum specific enthalpy over cells with R >= inner radius */
+static void torus_max_job(void *ctx, int k0, int k1, int slot)
+{
+    TorusMaxCtx *m = (TorusMaxCtx *)ctx;
+    double h = 1.0;
+    for (int k = k0; k <= k1; ++k)
+        for (int j = m->b->lo[1]; j <= m->b->hi[1]; ++j)
+            for (int i = m->b->lo[0]; i <= m->b->hi[0]; ++i)
+            {
+                double x, y, z;
+                cell_position(m->p, i, j, k, &x, &y, &z);
+                const double R = sqrt(x * x + y * y);
+                if (R < m->c->inner_radius)
+                    continue;
+                const double W =
+                    torus_potential(m->p, m->t, x, y, z, m->tp->ell, m->c);
+                h = dmax(h, torus_enthalpy(W, m->tp));
+            }
+    m->hmax[slot] = h;
+}
+
+typedef struct
+{
+    const orc_params *p;
+    const orc_torus_config *c;
+    const orc_torus_params *t;
+    const orc_box *b;
+    double *state;
+    double time;
+} TorusFillCtx;
+
+static void torus_fill_job(void *ctx, int k0, int k1, int slot);
+
 /* make_fixed_bg_torus_parameters, :291-331 (domain = the box interior) */
 int orc_make_torus_parameters(const orc_params *p, const orc_torus_config *c,
                               const orc_box *b, double t,
@@ -1930,19 +2061,16 @@ int orc_make_torus_parameters(const orc_params *p, const orc_torus_config *c,
         torus_potential(p, t, c->inner_radius, 0.0, 0.0, out->ell, c);
     if (!isfinite(out->surface_potential))
         return ORC_ERR_SETUP;
-    for (int k = b->lo[2]; k <= b->hi[2]; ++k)
-        for (int j = b->lo[1]; j <= b->hi[1]; ++j)
-            for (int i = b->lo[0]; i <= b->hi[0]; ++i)
-            {
-                double x, y, z;
-                cell_position(p, i, j, k, &x, &y, &z);
-                const double R = sqrt(x * x + y * y);
-                if (R < c->inner_radius)
-                    continue;
-                const double W = torus_potential(p, t, x, y, z, out->ell, c);
-                out->max_enthalpy = dmax(out->max_enthalpy,
-                                         torus_enthalpy(W, out));
-            }
+    TorusMaxCtx *mc = (TorusMaxCtx *)calloc(1, sizeof(TorusMaxCtx));
+    mc->p = p;
+    mc->c = c;
+    mc->b = b;
+    mc->t = t;
+    mc->tp = out;
+    const int n = parallel_z(b->lo[2], b->hi[2], torus_max_job, mc, 256);
+    for (int s = 0; s < n; ++s)
+        out->max_enthalpy = dmax(out->max_enthalpy, mc->hmax[s]);
+    free(mc);
     if (out->max_enthalpy <= 1.0)
         return ORC_ERR_SETUP;
     const double G = p->gamma;
@@ -1979,21 +2107,30 @@ int orc_fill_torus(const orc_params *p, const orc_torus_config *c,
                    const orc_torus_params *t, const orc_box *b,
                    double *state, double time)
 {
-    for (int k = b->glo[2]; k <= b->ghi[2]; ++k)
+    TorusFillCtx f = {p, c, t, b, state, time};
+    parallel_z(b->glo[2], b->ghi[2], torus_fill_job, &f, 256);
+    return ORC_OK;
+}
+
+static void torus_fill_job(void *ctx, int k0, int k1, int slot)
+{
+    (void)slot;
+    const TorusFillCtx *f = (const TorusFillCtx *)ctx;
+    const orc_box *b = f->b;
+    for (int k = k0; k <= k1; ++k)
         for (int j = b->glo[1]; j <= b->ghi[1]; ++j)
             for (int i = b->glo[0]; i <= b->ghi[0]; ++i)
             {
                 double x, y, z;
-                cell_position(p, i, j, k, &x, &y, &z);
+                cell_position(f->p, i, j, k, &x, &y, &z);
                 Geom g;
-                load_geometry(p, time, i, j, k, &g);
-                const Prim pr = torus_prim(p, x, y, &g, t, c);
+                load_geometry(f->p, f->time, i, j, k, &g);
+                const Prim pr = torus_prim(f->p, x, y, &g, f->t, f->c);
                 const int64_t idx = fab_index(b, i, j, k);
-                store_prim(b, state, idx, &pr);
-                const Cons cc = p2c(p->gamma, &pr, g.gLL);
-                store_cons(b, state, idx, &cc);
+                store_prim(b, f->state, idx, &pr);
+                const Cons cc = p2c(f->p->gamma, &pr, g.gLL);
+                store_cons(b, f->state, idx, &cc);
             }
-    return ORC_OK;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -2232,4 +2369,45 @@ void orc_disk_diagnostics(const orc_params *p, const orc_box *b,
     out[4] = mp;
     out[5] = mv;
     out[6] = mW;
+}
+
+/* Conserved variables of every cell of the ghosted box from the primitive
+ * components already stored there (the fixture fill of
+ * Tests/GRHDFixedBGTest/GRHDFixedBGTest.cpp:136-160). */
+typedef struct
+{
+    const orc_params *p;
+    const orc_box *b;
+    double *state;
+    double t;
+} ConsFillCtx;
+
+static void cons_fill_job(void *ctx, int k0, int k1, int slot);
+
+void orc_fill_conserved_from_primitives(const orc_params *p, const orc_box *b,
+                                        double *state, double t)
+{
+    ConsFillCtx f = {p, b, state, t};
+    parallel_z(b->glo[2], b->ghi[2], cons_fill_job, &f, 256);
+}
+
+static void cons_fill_job(void *ctx, int k0, int k1, int slot)
+{
+    (void)slot;
+    const ConsFillCtx *f = (const ConsFillCtx *)ctx;
+    const orc_params *p = f->p;
+    const orc_box *b = f->b;
+    double *state = f->state;
+    const double t = f->t;
+    for (int k = k0; k <= k1; ++k)
+        for (int j = b->glo[1]; j <= b->ghi[1]; ++j)
+            for (int i = b->glo[0]; i <= b->ghi[0]; ++i)
+            {
+                Geom g;
+                load_geometry(p, t, i, j, k, &g);
+                const int64_t idx = fab_index(b, i, j, k);
+                const Prim pr = load_prim(b, state, idx);
+                const Cons c = p2c(p->gamma, &pr, g.gLL);
+                store_cons(b, state, idx, &c);
+            }
 }

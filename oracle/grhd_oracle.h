@@ -208,6 +208,14 @@ int orc_michel_point(const orc_params *p, const orc_michel_config *c,
 int orc_fill_michel(const orc_params *p, const orc_michel_config *c,
                     const orc_box *box, double *state);
 
+/* Number of threads the setup passes (initial data, recovery) use. */
+void orc_set_threads(int n);
+
+/* conserved components of the whole ghosted box from its primitives */
+void orc_fill_conserved_from_primitives(const orc_params *p,
+                                        const orc_box *box, double *state,
+                                        double time);
+
 /* ---- diagnostics (example drivers) ---- */
 /* out: mass, disk_mass, tau, max_rho, max_pressure, max_velocity,
  * max_lorentz_factor (Main_GRHDLevelDataKerrSchildDisk.cpp:223-290) over

@@ -148,6 +148,9 @@ def lib():
         L.orc_michel_point.argtypes = [P, C.POINTER(MichelConfig), C.c_double,
                                        dp]
         L.orc_fill_michel.argtypes = [P, C.POINTER(MichelConfig), B, dp]
+        L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_fill_conserved_from_primitives.argtypes = [P, B, dp,
+                                                         C.c_double]
         L.orc_disk_diagnostics.argtypes = [P, B, C.c_int * 3, C.c_int * 3, dp,
                                            C.c_double, dp]
         _lib = L
@@ -365,6 +368,16 @@ def fill_michel(p, cfg, box, state):
                                _dp(state))
     if st:
         raise OracleError(st)
+
+
+def set_threads(n: int):
+    """Threads of the oracle's setup passes (initial data, recovery)."""
+    lib().orc_set_threads(int(n))
+
+
+def fill_conserved_from_primitives(p, box, state, time=0.0):
+    lib().orc_fill_conserved_from_primitives(C.byref(p), C.byref(box),
+                                             _dp(state), time)
 
 
 def disk_diagnostics(p, box, lo, hi, state, time=0.0) -> np.ndarray:
