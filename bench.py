@@ -154,9 +154,14 @@ def run_ours(args, rank, world, local_rank):
     if dist:
         import torch.distributed as tdist
 
+    # One step = the CFL speed of the current state + one RK4 step; the
+    # speed is computed inside the previous step's last stage (the first
+    # step computes it from the state).
+    cfl_state = {"mi": 0.0}
+
     def step(t):
-        dt = op.compute_stable_dt(lv, cfl=CFL, time=t)
-        op.advance_rk4(lv, time=t, dt=dt)
+        dt, cfl_state["mi"], _ = op.advance_rk4_cfl(
+            lv, CFL, time=t, max_inverse_dt=cfl_state["mi"])
         return t + dt
 
     t = 0.0

@@ -124,6 +124,9 @@ SIGNATURES = {
     "grhd_advance_rk4": (C.c_int, [_vp, _vp, C.c_int64, _P(Box), _dp,
                                    C.c_double, C.c_double, _P(Diagnostics),
                                    _vp]),
+    "grhd_advance_rk4_cfl": (C.c_int, [_vp, _vp, C.c_int64, _P(Box), _dp,
+                                       C.c_double, C.c_double, C.c_double,
+                                       _dp, _dp, _P(Diagnostics), _vp]),
     "grhd_eval_background": (C.c_int, [_vp, C.c_int64, _vp, C.c_double, _vp,
                                        _vp]),
     "grhd_eval_con2prim": (C.c_int, [_vp, C.c_int64, _vp, _vp, _vp, _vp, _vp,

@@ -362,14 +362,18 @@ void read_diag(const grhd_ctx *ctx, grhd_diagnostics *d)
     d->num_conserved_resets += (long long)ctx->status_h->counts[3];
 }
 
-// One RHS evaluation on the device (no synchronisation).
+// One RHS evaluation on the device (no synchronisation).  With
+// `prepared` the interior primitive cache and sources were already
+// written by the previous fused stage kernel for this state and time.
 void enqueue_rhs(grhd_ctx *ctx, double *rhs, double *state, const BoxDev &b,
-                 const Background &bg, const double inv_dx[3], cudaStream_t s)
+                 const Background &bg, const double inv_dx[3], cudaStream_t s,
+                 bool prepared = false)
 {
     {
         Timed t_(ctx, GRHD_K_GHOSTS, s);
-        launch_fill_ghosts(state, b, bg, ctx->opt, ctx->status, s);
+        launch_fill_ghosts(state, ctx->prim, b, bg, ctx->opt, ctx->status, s);
     }
+    if (!prepared)
     {
         Timed t_(ctx, GRHD_K_CELLS, s);
         launch_cells(state, ctx->prim, ctx->src, b, bg, ctx->opt, ctx->status,
@@ -687,52 +691,40 @@ int grhd_advance_ssprk2(grhd_ctx *ctx, double *state, int64_t state_cs,
     sb.cs = b.gvol();
     const Background bg0 = make_background(ctx->params, time);
     const Background bg1 = make_background(ctx->params, time + dt);
-    // rhs_initial = L(state); stage = state + dt rhs_initial, recovered
+    // rhs_initial = L(state); stage = state + dt rhs_initial recovered at
+    // t + dt, fused with the primitive cache and sources of L(stage)
     enqueue_rhs(ctx, ctx->kbuf, state, b, bg0, inverse_dx, s);
     {
-        // stage interior from state (different strides): update kernel
-        // reads `state` with stride b.cs and writes the stage with sb.cs.
-        // Both are indexed by the ghosted linear index, so use a strided
-        // copy of the 11 components first, then update in place.
-        GRHD_CUDA(ctx, cudaMemcpy2DAsync(ctx->stage, sb.cs * sizeof(double),
-                                         state, b.cs * sizeof(double),
-                                         b.gvol() * sizeof(double),
-                                         kStateComps,
-                                         cudaMemcpyDeviceToDevice, s));
+        Timed t_(ctx, GRHD_K_STAGE, s);
+        launch_stage(1, state, b.cs, nullptr, 0, ctx->stage, sb.cs, ctx->kbuf,
+                     nullptr, ctx->prim, ctx->src, b, bg1, ctx->opt, 0, dt,
+                     false, inverse_dx, ctx->status, s);
     }
+    // rhs_stage = L(stage) at t + dt, then the SSPRK2 combination
+    enqueue_rhs(ctx, ctx->kbuf, ctx->stage, sb, bg1, inverse_dx, s, true);
     {
         Timed t_(ctx, GRHD_K_STAGE, s);
-        launch_update(ctx->stage, sb.cs, ctx->stage, sb.cs, ctx->kbuf, sb,
-                      bg1, ctx->opt, dt, 1, ctx->status, s);
-    }
-    // rhs_stage = L(stage) at t + dt
-    enqueue_rhs(ctx, ctx->kbuf, ctx->stage, sb, bg1, inverse_dx, s);
-    {
-        Timed t_(ctx, GRHD_K_STAGE, s);
-        launch_ssprk2_combine(state, b.cs, ctx->stage, sb.cs, ctx->kbuf, b,
-                              bg1, ctx->opt, dt, ctx->status, s);
+        launch_stage(2, state, b.cs, ctx->stage, sb.cs, state, b.cs,
+                     ctx->kbuf, nullptr, nullptr, nullptr, b, bg1, ctx->opt,
+                     0, dt, false, inverse_dx, ctx->status, s);
     }
     st = finish_status(ctx, b, state, bg0, s);
     read_diag(ctx, diag);
     return st;
 }
 
-int grhd_advance_rk4(grhd_ctx *ctx, double *state, int64_t state_cs,
-                     const grhd_box *box, const double inverse_dx[3],
-                     double time, double dt, grhd_diagnostics *diag,
-                     void *stream)
+} // extern "C"
+
+namespace {
+
+// Classic RK4 (new): stage RHS times t, t+dt/2, t+dt/2, t+dt; every stage
+// combination is fused with the post-update recovery at the next RHS time
+// and with that RHS's per-cell work; the last stage optionally computes the
+// next CFL speed.  No host synchronisation.
+void enqueue_rk4(grhd_ctx *ctx, double *state, const BoxDev &b,
+                 const double inverse_dx[3], double time, double dt,
+                 bool want_cfl, cudaStream_t s)
 {
-    int st = common_checks(ctx, state, box);
-    if (st)
-        return st;
-    if (!inverse_dx || !box_is_domain(box))
-        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
-                         "advance needs the box to cover the whole domain");
-    cudaStream_t s = (cudaStream_t)stream;
-    const BoxDev b = make_box(box, state_cs);
-    if ((st = check_strides(ctx, b, state_cs, -1)) ||
-        (st = ensure_scratch(ctx, b, true)) || (st = reset_status(ctx, s)))
-        return st;
     BoxDev sb = b;
     sb.cs = b.gvol();
     const Background bgs[4] = {
@@ -740,35 +732,114 @@ int grhd_advance_rk4(grhd_ctx *ctx, double *state, int64_t state_cs,
         make_background(ctx->params, time + 0.5 * dt),
         make_background(ctx->params, time + 0.5 * dt),
         make_background(ctx->params, time + dt)};
-    const Background bg_rec[4] = {bgs[1], bgs[1], bgs[3], bgs[3]};
-    // the stage buffer starts as a copy of the state (its excised cells
-    // keep the frozen primitives)
-    GRHD_CUDA(ctx, cudaMemcpy2DAsync(ctx->stage, sb.cs * sizeof(double), state,
-                                     b.cs * sizeof(double),
-                                     b.gvol() * sizeof(double), kStateComps,
-                                     cudaMemcpyDeviceToDevice, s));
     for (int stage = 0; stage < 4; ++stage)
     {
         if (stage == 0)
             enqueue_rhs(ctx, ctx->kbuf, state, b, bgs[0], inverse_dx, s);
         else
             enqueue_rhs(ctx, ctx->kbuf, ctx->stage, sb, bgs[stage],
-                        inverse_dx, s);
-        // stages 0-2 write U^n + c dt k into the stage buffer; stage 3 writes
-        // U^{n+1} into the caller's state
+                        inverse_dx, s, true);
         Timed t_(ctx, GRHD_K_STAGE, s);
         if (stage < 3)
-            launch_rk4_stage(state, b.cs, ctx->stage, sb.cs, ctx->kbuf,
-                             ctx->acc, b, bg_rec[stage], ctx->opt, stage, dt,
-                             ctx->status, s);
+            launch_stage(0, state, b.cs, nullptr, 0, ctx->stage, sb.cs,
+                         ctx->kbuf, ctx->acc, ctx->prim, ctx->src, b,
+                         bgs[stage + 1], ctx->opt, stage, dt, false,
+                         inverse_dx, ctx->status, s);
         else
-            launch_rk4_stage(state, b.cs, state, b.cs, ctx->kbuf, ctx->acc, b,
-                             bg_rec[stage], ctx->opt, stage, dt, ctx->status,
-                             s);
+            launch_stage(0, state, b.cs, nullptr, 0, state, b.cs, ctx->kbuf,
+                         ctx->acc, nullptr, nullptr, b, bgs[3], ctx->opt,
+                         stage, dt, want_cfl, inverse_dx, ctx->status, s);
     }
-    st = finish_status(ctx, b, state, bgs[0], s);
+}
+
+int advance_checks(grhd_ctx *ctx, double *state, int64_t state_cs,
+                   const grhd_box *box, const double inverse_dx[3],
+                   BoxDev &b, cudaStream_t s)
+{
+    int st = common_checks(ctx, state, box);
+    if (st)
+        return st;
+    if (!inverse_dx || !box_is_domain(box))
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "advance needs the box to cover the whole domain");
+    b = make_box(box, state_cs);
+    if ((st = check_strides(ctx, b, state_cs, -1)) ||
+        (st = ensure_scratch(ctx, b, true)) || (st = reset_status(ctx, s)))
+        return st;
+    return GRHD_OK;
+}
+
+double bits_to_double(unsigned long long bits)
+{
+    double v;
+    std::memcpy(&v, &bits, sizeof(v));
+    return v;
+}
+
+} // namespace
+
+extern "C" {
+
+int grhd_advance_rk4(grhd_ctx *ctx, double *state, int64_t state_cs,
+                     const grhd_box *box, const double inverse_dx[3],
+                     double time, double dt, grhd_diagnostics *diag,
+                     void *stream)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    BoxDev b;
+    int st = advance_checks(ctx, state, state_cs, box, inverse_dx, b, s);
+    if (st)
+        return st;
+    enqueue_rk4(ctx, state, b, inverse_dx, time, dt, false, s);
+    st = finish_status(ctx, b, state, make_background(ctx->params, time), s);
     read_diag(ctx, diag);
     return st;
+}
+
+int grhd_advance_rk4_cfl(grhd_ctx *ctx, double *state, int64_t state_cs,
+                         const grhd_box *box, const double inverse_dx[3],
+                         double time, double cfl, double max_dt,
+                         double *max_inverse_dt, double *dt_used,
+                         grhd_diagnostics *diag, void *stream)
+{
+    if (ctx && (!(cfl > 0.0) || !max_inverse_dt))
+    {
+        std::memset(&ctx->last_error, 0, sizeof(ctx->last_error));
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "GRHD CFL number must be positive");
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    BoxDev b;
+    int st = advance_checks(ctx, state, state_cs, box, inverse_dx, b, s);
+    if (st)
+        return st;
+    const Background bg0 = make_background(ctx->params, time);
+    double mi = *max_inverse_dt;
+    if (!(mi > 0.0))
+    {
+        {
+            Timed t_(ctx, GRHD_K_CFL, s);
+            launch_max_inv_dt(state, b, bg0, ctx->opt, inverse_dx,
+                              ctx->status, s);
+        }
+        if ((st = finish_status(ctx, b, state, bg0, s)))
+            return st;
+        mi = bits_to_double(ctx->status_h->maxinv_bits);
+        if ((st = reset_status(ctx, s)))
+            return st;
+    }
+    double dt = cfl / std::fmax(mi, 1.0e-14);
+    if (max_dt > 0.0)
+        dt = std::fmin(dt, max_dt);
+    enqueue_rk4(ctx, state, b, inverse_dx, time, dt, true, s);
+    st = finish_status(ctx, b, state, bg0, s);
+    read_diag(ctx, diag);
+    if (st)
+        return st;
+    *max_inverse_dt = bits_to_double(ctx->status_h->maxinv_bits);
+    if (dt_used)
+        *dt_used = dt;
+    return GRHD_OK;
 }
 
 int grhd_eval_background(grhd_ctx *ctx, int64_t n, const double *xyz,

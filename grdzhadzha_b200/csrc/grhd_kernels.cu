@@ -83,13 +83,6 @@ __device__ __forceinline__ bool primitive_differs(const Prim &a, const Prim &b)
            a.v[0] != b.v[0] || a.v[1] != b.v[1] || a.v[2] != b.v[2];
 }
 
-__device__ __forceinline__ bool is_interior(const BoxDev &b, int i, int j,
-                                            int k)
-{
-    return i >= b.lo[0] && i <= b.hi[0] && j >= b.lo[1] && j <= b.hi[1] &&
-           k >= b.lo[2] && k <= b.hi[2];
-}
-
 // ------------------------------------------------------------ ghost fill
 
 // Enumerates the shell "ghosted box minus interior box" as three slabs:
@@ -140,9 +133,24 @@ __device__ __forceinline__ bool shell_cell(const BoxDev &b, int64_t t, int &i,
     return false;
 }
 
+__device__ __forceinline__ void store_pv(double *prim, int64_t pcs,
+                                         int64_t g, const Prim &pr)
+{
+    prim[0 * pcs + g] = pr.rho;
+    prim[1 * pcs + g] = pr.p;
+    prim[2 * pcs + g] = pr.v[0];
+    prim[3 * pcs + g] = pr.v[1];
+    prim[4 * pcs + g] = pr.v[2];
+}
+
+// Physical (outflow) ghost fill of the shell "ghosted box minus box"
+// (fill_conserved_outflow_boundaries_from_fixed_background, :113-177),
+// then, for every shell cell, the ghosted-box con2prim of the RHS into the
+// primitive cache (recover_primitives_from_fixed_background, :33-58).
 __global__ void __launch_bounds__(256)
-    k_fill_ghosts(double *__restrict__ state, BoxDev b, Background bg,
-                  Options o, DevStatus *st, int64_t nshell)
+    k_fill_ghosts(double *__restrict__ state, double *__restrict__ prim,
+                  BoxDev b, Background bg, Options o, DevStatus *st,
+                  int64_t nshell)
 {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
          t < nshell; t += (int64_t)gridDim.x * blockDim.x)
@@ -151,7 +159,7 @@ __global__ void __launch_bounds__(256)
         if (!shell_cell(b, t, i, j, k))
             continue;
         const int iv[3] = {i, j, k};
-        int src[3] = {i, j, k};
+        int srcc[3] = {i, j, k};
         bool ghost = false;
 #pragma unroll
         for (int d = 0; d < 3; ++d)
@@ -159,124 +167,146 @@ __global__ void __launch_bounds__(256)
             if (iv[d] < b.dlo[d])
             {
                 ghost = true;
-                src[d] = b.lo[d];
+                srcc[d] = b.lo[d];
             }
             else if (iv[d] > b.dhi[d])
             {
                 ghost = true;
-                src[d] = b.hi[d];
+                srcc[d] = b.hi[d];
             }
         }
-        if (!ghost)
-            continue;
         double x, y, z;
-        cell_xyz(o, src[0], src[1], src[2], x, y, z);
-        Geo sg;
-        background_metric<false>(bg, x, y, z, sg, nullptr);
-        const Cons sc =
-            load_cons(state, b.cs, b.gidx(src[0], src[1], src[2]));
-        Prim pr;
-        if (!con2prim(o, sc, sg.gUU, pr, nullptr, nullptr))
-        {
-            record_error(st, 1, b.gidx(i, j, k));
-            continue;
-        }
+        const int64_t idx = b.gidx(i, j, k);
         cell_xyz(o, i, j, k, x, y, z);
         Geo tg;
         background_metric<false>(bg, x, y, z, tg, nullptr);
-        floors(o, pr, tg.gLL);
-        const int64_t idx = b.gidx(i, j, k);
-        store_prim(state, b.cs, idx, pr);
-        store_cons(state, b.cs, idx, p2c(pr, tg.gLL));
+        Cons c;
+        if (ghost)
+        {
+            double sx, sy, sz;
+            cell_xyz(o, srcc[0], srcc[1], srcc[2], sx, sy, sz);
+            Geo sg;
+            background_metric<false>(bg, sx, sy, sz, sg, nullptr);
+            const Cons sc =
+                load_cons(state, b.cs, b.gidx(srcc[0], srcc[1], srcc[2]));
+            Prim pr;
+            if (!con2prim(o, sc, sg.gUU, pr, nullptr, nullptr))
+            {
+                record_error(st, 1, idx);
+                continue;
+            }
+            floors(o, pr, tg.gLL);
+            store_prim(state, b.cs, idx, pr);
+            c = p2c(pr, tg.gLL);
+            store_cons(state, b.cs, idx, c);
+        }
+        else
+            c = load_cons(state, b.cs, idx);
+        Prim pr;
+        if (!con2prim(o, c, tg.gUU, pr, nullptr, nullptr))
+        {
+            record_error(st, 2, idx);
+            pr.rho = pr.p = 1.0;
+            pr.v[0] = pr.v[1] = pr.v[2] = 0.0;
+        }
+        store_pv(prim, b.pcs, idx, pr);
     }
+}
+
+// Static-metric sources (:255-298) from the floored primitives and, for
+// the binary, the volume-time source (:616-675); `pr` is the cell's
+// unfloored con2prim result.
+__device__ __forceinline__ Cons cell_sources(const Options &o,
+                                             const Background &bg, double x,
+                                             double y, double z,
+                                             const Prim &pr, const Cons &c,
+                                             const GeoFull &f)
+{
+    Cons s;
+    s.D = s.tau = s.S[0] = s.S[1] = s.S[2] = 0.0;
+    if (o.use_src)
+    {
+        Prim fp = pr;
+        floors(o, fp, f.g.gLL);
+        if (!is_atmo(o, fp, o.src_atmo_factor))
+            s = static_sources(fp, c, f);
+    }
+    if (o.use_vol && bg.kind == 1)
+    {
+        const double pos[3] = {x, y, z};
+        const double Up = pn_scalar(bg.m1, bg.m2, bg.soft2, bg.p1p, bg.p2p, pos);
+        const double Um = pn_scalar(bg.m1, bg.m2, bg.soft2, bg.p1m, bg.p2m, pos);
+        const double dl =
+            __dadd_rn(pn_log_sqrt_det(__dadd_rn(1.0, 2.0 * Up)),
+                      -pn_log_sqrt_det(__dadd_rn(1.0, 2.0 * Um))) /
+            (2.0 * bg.fd_h);
+        s.D += 0.0 - c.D * dl;
+        s.tau += 0.0 - c.tau * dl;
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+            s.S[m] += 0.0 - c.S[m] * dl;
+    }
+    return s;
+}
+
+__device__ __forceinline__ void store_src(double *src, int64_t rcs,
+                                          int64_t ri, const Cons &s)
+{
+    src[0 * rcs + ri] = s.D;
+    src[1 * rcs + ri] = s.S[0];
+    src[2 * rcs + ri] = s.S[1];
+    src[3 * rcs + ri] = s.S[2];
+    src[4 * rcs + ri] = s.tau;
 }
 
 // ------------------------------------------------------- per-cell pass
 
-__global__ void __launch_bounds__(256)
+// Interior cells: con2prim into the primitive cache (the ghosted-box
+// recovery of the RHS restricted to the interior; the shell is done by
+// k_fill_ghosts) and the sources into the source scratch.  Excised cells
+// keep their frozen primitives and get no source.
+__global__ void __launch_bounds__(256, 2)
     k_cells(const double *__restrict__ state, double *__restrict__ prim,
             double *__restrict__ src, BoxDev b, Background bg, Options o,
             DevStatus *st)
 {
-    const int64_t n = b.gvol();
+    const int64_t n = b.ivol();
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
          t += (int64_t)gridDim.x * blockDim.x)
     {
-        const int i = b.glo[0] + (int)(t % b.gn[0]);
-        const int64_t r = t / b.gn[0];
-        const int j = b.glo[1] + (int)(r % b.gn[1]);
-        const int k = b.glo[2] + (int)(r / b.gn[1]);
-        const bool inner = is_interior(b, i, j, k);
-        if (inner && excised(o, i, j, k))
+        const int i = b.lo[0] + (int)(t % b.in[0]);
+        const int64_t r = t / b.in[0];
+        const int j = b.lo[1] + (int)(r % b.in[1]);
+        const int k = b.lo[2] + (int)(r / b.in[1]);
+        const int64_t g = b.gidx(i, j, k);
+        Cons s;
+        s.D = s.tau = s.S[0] = s.S[1] = s.S[2] = 0.0;
+        if (excised(o, i, j, k))
         {
-            const Prim pr = load_prim(state, b.cs, t);
-            prim[0 * b.pcs + t] = pr.rho;
-            prim[1 * b.pcs + t] = pr.p;
-            prim[2 * b.pcs + t] = pr.v[0];
-            prim[3 * b.pcs + t] = pr.v[1];
-            prim[4 * b.pcs + t] = pr.v[2];
-            const int64_t ri = b.iidx(i, j, k);
-#pragma unroll
-            for (int c = 0; c < 5; ++c)
-                src[c * b.rcs + ri] = 0.0;
+            store_pv(prim, b.pcs, g, load_prim(state, b.cs, g));
+            store_src(src, b.rcs, t, s);
             continue;
         }
         double x, y, z;
         cell_xyz(o, i, j, k, x, y, z);
-        const bool want_src = inner && (o.use_src || o.use_vol);
         GeoFull f;
-        if (inner && o.use_src)
+        if (o.use_src)
             background_metric<true>(bg, x, y, z, f.g, &f);
         else
             background_metric<false>(bg, x, y, z, f.g, nullptr);
-        const Cons c = load_cons(state, b.cs, t);
+        const Cons c = load_cons(state, b.cs, g);
         Prim pr;
         if (!con2prim(o, c, f.g.gUU, pr, nullptr, nullptr))
         {
-            record_error(st, 2, t);
+            record_error(st, 2, g);
             pr.rho = pr.p = 1.0;
             pr.v[0] = pr.v[1] = pr.v[2] = 0.0;
             pr.eps = 1.0;
         }
-        prim[0 * b.pcs + t] = pr.rho;
-        prim[1 * b.pcs + t] = pr.p;
-        prim[2 * b.pcs + t] = pr.v[0];
-        prim[3 * b.pcs + t] = pr.v[1];
-        prim[4 * b.pcs + t] = pr.v[2];
-        if (!inner)
-            continue;
-        Cons s;
-        s.D = s.tau = s.S[0] = s.S[1] = s.S[2] = 0.0;
-        if (want_src && o.use_src)
-        {
-            Prim fp = pr;
-            floors(o, fp, f.g.gLL);
-            if (!is_atmo(o, fp, o.src_atmo_factor))
-                s = static_sources(fp, c, f);
-        }
-        if (want_src && o.use_vol && bg.kind == 1)
-        {
-            const double pos[3] = {x, y, z};
-            const double Up =
-                pn_scalar(bg.m1, bg.m2, bg.soft2, bg.p1p, bg.p2p, pos);
-            const double Um =
-                pn_scalar(bg.m1, bg.m2, bg.soft2, bg.p1m, bg.p2m, pos);
-            const double dl =
-                __dadd_rn(pn_log_sqrt_det(__dadd_rn(1.0, 2.0 * Up)),
-                          -pn_log_sqrt_det(__dadd_rn(1.0, 2.0 * Um))) /
-                (2.0 * bg.fd_h);
-            s.D += 0.0 - c.D * dl;
-            s.tau += 0.0 - c.tau * dl;
-#pragma unroll
-            for (int m = 0; m < 3; ++m)
-                s.S[m] += 0.0 - c.S[m] * dl;
-        }
-        const int64_t ri = b.iidx(i, j, k);
-        src[0 * b.rcs + ri] = s.D;
-        src[1 * b.rcs + ri] = s.S[0];
-        src[2 * b.rcs + ri] = s.S[1];
-        src[3 * b.rcs + ri] = s.S[2];
-        src[4 * b.rcs + ri] = s.tau;
+        else
+            s = cell_sources(o, bg, x, y, z, pr, c, f);
+        store_pv(prim, b.pcs, g, pr);
+        store_src(src, b.rcs, t, s);
     }
 }
 
@@ -668,71 +698,72 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// combine_ssprk2_conserved_state (FArrayBoxFiniteVolume.hpp:942-969) with
-// the final recover_primitives fused in: U = (U^n + U^1 + dt L(U^1)) / 2.
-__global__ void __launch_bounds__(256)
-    k_ssprk2_combine(double *__restrict__ state, int64_t scs,
-                     const double *__restrict__ stage, int64_t tcs,
-                     const double *__restrict__ rhs, BoxDev b, Background bg,
-                     Options o, double dt, DevStatus *st)
+// Characteristic-speed CFL contribution of one cell, sum_d max|lambda|/dx_d
+// (compute_max_inverse_dt_from_fixed_background, :398-409) for floored
+// primitives that are not atmosphere.
+__device__ __forceinline__ double cell_inverse_dt(const Options &o,
+                                                  const Prim &fp,
+                                                  const Geo &g,
+                                                  const double inv[3])
 {
-    unsigned long long cnt[4] = {0, 0, 0, 0};
-    const int64_t n = b.ivol();
-    const int64_t n_pad = (n + blockDim.x - 1) / blockDim.x * blockDim.x;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_pad;
-         t += (int64_t)gridDim.x * blockDim.x)
+    double cell = 0.0;
+    if (!is_atmo(o, fp, 1.0 + 1.0e-12))
     {
-        if (t < n)
-        {
-            int i, j, k;
-            interior_cell(b, t, i, j, k);
-            if (!excised(o, i, j, k))
-            {
-                const int64_t g = b.gidx(i, j, k);
-                const int comp_of[5] = {kD, kS1, kS1 + 1, kS1 + 2, kTau};
-                double u[5];
 #pragma unroll
-                for (int c = 0; c < 5; ++c)
-                {
-                    const int q = comp_of[c];
-                    u[c] = 0.5 * (state[q * scs + g] + stage[q * tcs + g] +
-                                  dt * rhs[c * b.rcs + t]);
-                }
-                Cons c;
-                c.D = u[0];
-                c.S[0] = u[1];
-                c.S[1] = u[2];
-                c.S[2] = u[3];
-                c.tau = u[4];
-                double x, y, z;
-                cell_xyz(o, i, j, k, x, y, z);
-                Geo geo;
-                background_metric<false>(bg, x, y, z, geo, nullptr);
-                recover_cell(o, geo, c, state, scs, g, cnt);
-            }
+        for (int d = 0; d < 3; ++d)
+        {
+            double lo, hi;
+            char_speeds(o, fp, g, d, lo, hi);
+            cell += fmax(fabs(lo), fabs(hi)) * inv[d];
         }
-        flush_counts(st, cnt);
-        cnt[0] = cnt[1] = cnt[2] = cnt[3] = 0;
     }
+    return cell;
 }
 
-// One RK4 stage combination + post-stage recovery (new).  stage 0..2:
-// out = U^n + c_s dt k_s with acc accumulating k1 + 2k2 + 2k3; stage 3:
-// out = U^n + dt/6 (acc + k4).
-__global__ void __launch_bounds__(256)
-    k_rk4_stage(const double *un, int64_t ucs, double *out, int64_t ocs,
-                const double *__restrict__ kv, double *__restrict__ acc,
-                BoxDev b, Background bg, Options o, int stage, double dt,
-                DevStatus *st)
+__device__ __forceinline__ void flush_max(DevStatus *st, double v)
+{
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+        v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
+    if ((threadIdx.x & 31) == 0 && v > 0.0)
+        atomicMax(&st->maxinv_bits, (unsigned long long)__double_as_longlong(v));
+}
+
+// One stage of an integrator fused with the post-update recovery
+// (update_conserved / recover_primitives_and_apply_atmosphere,
+// FixedBGFArrayBoxFiniteVolume.hpp:60-110, 522-533) and, optionally, with
+// the per-cell work of the next RHS evaluation and of the next CFL speed,
+// which both start from con2prim of the state this stage writes:
+//   * prep: the next RHS's con2prim (unfloored, :33-58) into the primitive
+//     cache and its sources (:255-298, :616-675) into the source scratch;
+//   * cfl : the next compute_max_inverse_dt (:364-412) as a device max.
+// For a cell whose conserved variables were reset, the next con2prim runs
+// on the reset state, as the reference's next call would.
+// Modes: 0 RK4 stage `stage` (new): stages 0..2 out = U^n + c dt k with
+// acc = k1 (+ 2 k2 + 2 k3), stage 3 out = U^n + dt/6 (acc + k4);
+// 1 Euler update out = U^n + dt k (advance_ssprk2 stage, :578);
+// 2 SSPRK2 combine out = (U^n + U^1 + dt k)/2 (FArrayBoxFiniteVolume.hpp:
+// 942-969).
+template <int MODE>
+__global__ void __launch_bounds__(256, 2)
+    k_stage(const double *un, int64_t ucs, const double *us, int64_t tcs,
+            double *out, int64_t ocs, const double *__restrict__ kv,
+            double *__restrict__ acc, double *__restrict__ prim,
+            double *__restrict__ src, BoxDev b, Background bg, Options o,
+            int stage, double dt, int cfl, double i0, double i1, double i2,
+            DevStatus *st)
 {
     unsigned long long cnt[4] = {0, 0, 0, 0};
     const int64_t n = b.ivol();
     const int64_t n_pad = (n + blockDim.x - 1) / blockDim.x * blockDim.x;
     const double cst = (stage == 2) ? dt : 0.5 * dt;
     const double dt6 = dt / 6.0;
+    const double inv[3] = {i0, i1, i2};
+    const bool prep = prim != nullptr;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_pad;
          t += (int64_t)gridDim.x * blockDim.x)
     {
+        double cell_inv = 0.0;
         if (t < n)
         {
             int i, j, k;
@@ -743,6 +774,13 @@ __global__ void __launch_bounds__(256)
                 if (out != un)
                     for (int c = 0; c < kStateComps; ++c)
                         out[c * ocs + g] = un[c * ucs + g];
+                if (prep)
+                {
+                    store_pv(prim, b.pcs, g, load_prim(un, ucs, g));
+                    Cons z0;
+                    z0.D = z0.tau = z0.S[0] = z0.S[1] = z0.S[2] = 0.0;
+                    store_src(src, b.rcs, t, z0);
+                }
             }
             else
             {
@@ -753,20 +791,23 @@ __global__ void __launch_bounds__(256)
                 {
                     const double kk = kv[c * b.rcs + t];
                     const double u0 = un[comp_of[c] * ucs + g];
-                    double a = 0.0;
-                    if (stage == 0)
-                        a = kk;
-                    else
-                        a = acc[c * b.rcs + t];
-                    if (stage == 1 || stage == 2)
-                        a = a + 2.0 * kk;
-                    if (stage < 3)
+                    if (MODE == 0)
                     {
-                        acc[c * b.rcs + t] = a;
-                        u[c] = u0 + cst * kk;
+                        double a = (stage == 0) ? kk : acc[c * b.rcs + t];
+                        if (stage == 1 || stage == 2)
+                            a = a + 2.0 * kk;
+                        if (stage < 3)
+                        {
+                            acc[c * b.rcs + t] = a;
+                            u[c] = u0 + cst * kk;
+                        }
+                        else
+                            u[c] = u0 + dt6 * (a + kk);
                     }
+                    else if (MODE == 1)
+                        u[c] = u0 + dt * kk;
                     else
-                        u[c] = u0 + dt6 * (a + kk);
+                        u[c] = 0.5 * (u0 + us[comp_of[c] * tcs + g] + dt * kk);
                 }
                 Cons c;
                 c.D = u[0];
@@ -776,13 +817,75 @@ __global__ void __launch_bounds__(256)
                 c.tau = u[4];
                 double x, y, z;
                 cell_xyz(o, i, j, k, x, y, z);
-                Geo geo;
-                background_metric<false>(bg, x, y, z, geo, nullptr);
-                recover_cell(o, geo, c, out, ocs, g, cnt);
+                GeoFull f;
+                if (prep && o.use_src)
+                    background_metric<true>(bg, x, y, z, f.g, &f);
+                else
+                    background_metric<false>(bg, x, y, z, f.g, nullptr);
+                // recovery with atmosphere (:60-110)
+                Prim pr;
+                const bool ok = con2prim(o, c, f.g.gUU, pr, nullptr, nullptr);
+                bool reset = !ok;
+                Prim stored;
+                cnt[0] += 1;
+                if (ok)
+                {
+                    stored = pr;
+                    floors(o, stored, f.g.gLL);
+                    reset = primitive_differs(pr, stored);
+                    if (reset)
+                        cnt[2] += 1;
+                }
+                else
+                {
+                    cnt[1] += 1;
+                    stored = atmosphere(o);
+                }
+                if (reset)
+                {
+                    cnt[3] += 1;
+                    c = p2c(stored, f.g.gLL);
+                }
+                store_prim(out, ocs, g, stored);
+                store_cons(out, ocs, g, c);
+                if (prep || cfl)
+                {
+                    // con2prim of the state just written (unchanged cells:
+                    // the same solve on the same input gives pr again)
+                    Prim pn = pr;
+                    bool okn = ok;
+                    if (reset)
+                        okn = con2prim(o, c, f.g.gUU, pn, nullptr, nullptr);
+                    if (!okn)
+                    {
+                        record_error(st, cfl && !prep ? 4 : 2,
+                                     cfl && !prep ? t : g);
+                        pn.rho = pn.p = 1.0;
+                        pn.v[0] = pn.v[1] = pn.v[2] = 0.0;
+                        pn.eps = 1.0;
+                    }
+                    if (prep)
+                    {
+                        store_pv(prim, b.pcs, g, pn);
+                        Cons s;
+                        s.D = s.tau = s.S[0] = s.S[1] = s.S[2] = 0.0;
+                        if (okn)
+                            s = cell_sources(o, bg, x, y, z, pn, c, f);
+                        store_src(src, b.rcs, t, s);
+                    }
+                    if (cfl && okn)
+                    {
+                        Prim fp = pn;
+                        floors(o, fp, f.g.gLL);
+                        cell_inv = cell_inverse_dt(o, fp, f.g, inv);
+                    }
+                }
             }
         }
         flush_counts(st, cnt);
         cnt[0] = cnt[1] = cnt[2] = cnt[3] = 0;
+        if (cfl)
+            flush_max(st, cell_inv);
     }
 }
 
@@ -813,31 +916,15 @@ __global__ void __launch_bounds__(256)
                 Prim pr;
                 if (!con2prim(o, load_cons(state, b.cs, b.gidx(i, j, k)),
                               geo.gUU, pr, nullptr, nullptr))
-                {
                     record_error(st, 4, t);
-                }
                 else
                 {
                     floors(o, pr, geo.gLL);
-                    if (!is_atmo(o, pr, 1.0 + 1.0e-12))
-                    {
-#pragma unroll
-                        for (int d = 0; d < 3; ++d)
-                        {
-                            double lo, hi;
-                            char_speeds(o, pr, geo, d, lo, hi);
-                            cell += fmax(fabs(lo), fabs(hi)) * inv[d];
-                        }
-                    }
+                    cell = cell_inverse_dt(o, pr, geo, inv);
                 }
             }
         }
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1)
-            cell = fmax(cell, __shfl_down_sync(0xffffffffu, cell, off));
-        if ((threadIdx.x & 31) == 0 && cell > 0.0)
-            atomicMax(&st->maxinv_bits,
-                      (unsigned long long)__double_as_longlong(cell));
+        flush_max(st, cell);
     }
 }
 
@@ -950,21 +1037,22 @@ size_t face_kernel_smem_bytes()
            (5 * kPW * kPW + 2 * kGeoFields * kGW * kGW + 2 * 5 * kTB * kTC);
 }
 
-void launch_fill_ghosts(double *state, const BoxDev &b, const Background &bg,
-                        const Options &o, DevStatus *st, cudaStream_t s)
+void launch_fill_ghosts(double *state, double *prim, const BoxDev &b,
+                        const Background &bg, const Options &o, DevStatus *st,
+                        cudaStream_t s)
 {
     const int64_t nshell = b.gvol() - b.ivol();
     if (nshell <= 0)
         return;
-    k_fill_ghosts<<<grid_for(nshell, 256), 256, 0, s>>>(state, b, bg, o, st,
-                                                       nshell);
+    k_fill_ghosts<<<grid_for(nshell, 256), 256, 0, s>>>(state, prim, b, bg, o,
+                                                       st, nshell);
 }
 
 void launch_cells(const double *state, double *prim, double *src,
                   const BoxDev &b, const Background &bg, const Options &o,
                   DevStatus *st, cudaStream_t s)
 {
-    k_cells<<<grid_for(b.gvol(), 256), 256, 0, s>>>(state, prim, src, b, bg,
+    k_cells<<<grid_for(b.ivol(), 256), 256, 0, s>>>(state, prim, src, b, bg,
                                                     o, st);
 }
 
@@ -997,22 +1085,28 @@ void launch_recover(double *state, const BoxDev &b, const Background &bg,
     k_recover<<<grid_for(b.ivol(), 256), 256, 0, s>>>(state, b, bg, o, st);
 }
 
-void launch_ssprk2_combine(double *state, int64_t scs, const double *stage,
-                           int64_t tcs, const double *rhs, const BoxDev &b,
-                           const Background &bg, const Options &o, double dt,
-                           DevStatus *st, cudaStream_t s)
+void launch_stage(int mode, const double *un, int64_t ucs, const double *us,
+                  int64_t tcs, double *out, int64_t ocs, const double *k,
+                  double *acc, double *prim, double *src, const BoxDev &b,
+                  const Background &bg, const Options &o, int stage,
+                  double dt, bool cfl, const double inv_dx[3], DevStatus *st,
+                  cudaStream_t s)
 {
-    k_ssprk2_combine<<<grid_for(b.ivol(), 256), 256, 0, s>>>(
-        state, scs, stage, tcs, rhs, b, bg, o, dt, st);
-}
-
-void launch_rk4_stage(const double *un, int64_t ucs, double *out,
-                      int64_t ocs, const double *k, double *acc,
-                      const BoxDev &b, const Background &bg, const Options &o,
-                      int stage, double dt, DevStatus *st, cudaStream_t s)
-{
-    k_rk4_stage<<<grid_for(b.ivol(), 256), 256, 0, s>>>(
-        un, ucs, out, ocs, k, acc, b, bg, o, stage, dt, st);
+    const int grid = grid_for(b.ivol(), 256);
+    const double i0 = inv_dx ? inv_dx[0] : 0.0, i1 = inv_dx ? inv_dx[1] : 0.0,
+                 i2 = inv_dx ? inv_dx[2] : 0.0;
+    if (mode == 0)
+        k_stage<0><<<grid, 256, 0, s>>>(un, ucs, us, tcs, out, ocs, k, acc,
+                                        prim, src, b, bg, o, stage, dt,
+                                        cfl ? 1 : 0, i0, i1, i2, st);
+    else if (mode == 1)
+        k_stage<1><<<grid, 256, 0, s>>>(un, ucs, us, tcs, out, ocs, k, acc,
+                                        prim, src, b, bg, o, stage, dt,
+                                        cfl ? 1 : 0, i0, i1, i2, st);
+    else
+        k_stage<2><<<grid, 256, 0, s>>>(un, ucs, us, tcs, out, ocs, k, acc,
+                                        prim, src, b, bg, o, stage, dt,
+                                        cfl ? 1 : 0, i0, i1, i2, st);
 }
 
 void launch_max_inv_dt(const double *state, const BoxDev &b,

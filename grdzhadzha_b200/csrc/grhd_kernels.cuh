@@ -75,8 +75,12 @@ size_t face_kernel_smem_bytes();
 // Per-device kernel attributes (dynamic shared memory of the face kernel).
 cudaError_t configure_kernels();
 
-void launch_fill_ghosts(double *state, const BoxDev &b, const Background &bg,
-                        const Options &o, DevStatus *st, cudaStream_t s);
+// Physical ghost fill of the shell, then con2prim of every shell cell into
+// the primitive cache.
+void launch_fill_ghosts(double *state, double *prim, const BoxDev &b,
+                        const Background &bg, const Options &o, DevStatus *st,
+                        cudaStream_t s);
+// Interior con2prim into the primitive cache + sources.
 void launch_cells(const double *state, double *prim, double *src,
                   const BoxDev &b, const Background &bg, const Options &o,
                   DevStatus *st, cudaStream_t s);
@@ -92,14 +96,16 @@ void launch_update(double *dst, int64_t dcs, const double *src_state,
                    int recover, DevStatus *st, cudaStream_t s);
 void launch_recover(double *state, const BoxDev &b, const Background &bg,
                     const Options &o, DevStatus *st, cudaStream_t s);
-void launch_ssprk2_combine(double *state, int64_t scs, const double *stage,
-                           int64_t tcs, const double *rhs, const BoxDev &b,
-                           const Background &bg, const Options &o, double dt,
-                           DevStatus *st, cudaStream_t s);
-void launch_rk4_stage(const double *un, int64_t ucs, double *out,
-                      int64_t ocs, const double *k, double *acc,
-                      const BoxDev &b, const Background &bg, const Options &o,
-                      int stage, double dt, DevStatus *st, cudaStream_t s);
+// Integrator stage fused with the post-update recovery; mode 0 RK4 stage
+// `stage`, 1 Euler update, 2 SSPRK2 combine.  With prim/src non-null the
+// stage also prepares the next RHS (primitive cache and sources); with cfl
+// it accumulates the next max inverse dt into st->maxinv_bits.
+void launch_stage(int mode, const double *un, int64_t ucs, const double *us,
+                  int64_t tcs, double *out, int64_t ocs, const double *k,
+                  double *acc, double *prim, double *src, const BoxDev &b,
+                  const Background &bg, const Options &o, int stage,
+                  double dt, bool cfl, const double inv_dx[3], DevStatus *st,
+                  cudaStream_t s);
 void launch_max_inv_dt(const double *state, const BoxDev &b,
                        const Background &bg, const Options &o,
                        const double inv_dx[3], DevStatus *st, cudaStream_t s);

@@ -344,6 +344,24 @@ class _OperatorBase:
         return self._advance(self._lib.grhd_advance_rk4, state, inverse_dx_U,
                              time, dt)
 
+    def advance_rk4_cfl(self, state, cfl, time=0.0, max_dt=0.0,
+                        max_inverse_dt=0.0, inverse_dx_U=None):
+        """New: one RK4 step with dt = min(cfl / max_inverse_dt, max_dt),
+        the driver pattern compute_stable_dt + advance.  Pass the
+        max_inverse_dt this method returned for the same unmodified state
+        (0 recomputes it).  Returns (dt, next max_inverse_dt, diagnostics)."""
+        if not cfl > 0.0:
+            raise L.InvalidArgument(L.GRHD_ERR_INVALID_ARG, None)
+        mi = C.c_double(max_inverse_dt)
+        dt = C.c_double()
+        d = L.Diagnostics()
+        b = state.c_box()
+        self._check(self._lib.grhd_advance_rk4_cfl(
+            self._ctx, _ptr(state.state), state.comp_stride(), C.byref(b),
+            self._inv(inverse_dx_U), time, cfl, max_dt, C.byref(mi),
+            C.byref(dt), C.byref(d), _stream()))
+        return dt.value, mi.value, d
+
 
 class FixedBGLevelDataFiniteVolumeOperator(_OperatorBase):
     """FixedBGFArrayBoxFiniteVolume.hpp:446-614 (static background)."""

@@ -195,6 +195,20 @@ int grhd_advance_rk4(grhd_ctx *ctx, double *state, int64_t state_comp_stride,
                      double time, double dt, grhd_diagnostics *diag,
                      void *stream);
 
+/* New: one RK4 step whose dt comes from the CFL condition, as a driver's
+ * compute_stable_dt + advance pair does (dt = min(cfl / max_inverse_dt,
+ * max_dt); max_dt <= 0 means no cap).  *max_inverse_dt is in/out: pass the
+ * value this call returned for the same, unmodified state (or <= 0 to have
+ * it computed from `state` first); on return it holds the max inverse dt
+ * of the new state, computed inside the step's last stage.  *dt_used (may
+ * be NULL) receives the step taken. */
+int grhd_advance_rk4_cfl(grhd_ctx *ctx, double *state,
+                         int64_t state_comp_stride, const grhd_box *box,
+                         const double inverse_dx[3], double time, double cfl,
+                         double max_dt, double *max_inverse_dt,
+                         double *dt_used, grhd_diagnostics *diag,
+                         void *stream);
+
 /* ---- pointwise kernels for verification ---- */
 
 /* ADM background vars at n points (xyz[3n], positions relative to the

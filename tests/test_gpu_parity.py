@@ -119,6 +119,29 @@ def test_one_step_matches_oracle(name, method, G):
     assert np.all(full[5:] <= 1e-10), full
 
 
+@pytest.mark.parametrize("name", ["torus_a09", "michel_c1", "pndisk"])
+def test_rk4_cfl_steps_match_oracle(name, G):
+    """advance_rk4_cfl == compute_stable_dt + advance_rk4 for consecutive
+    steps; the max inverse dt handed from one step to the next is the one
+    its last stage computed."""
+    p, box, s, t = cases.CASES[name]()
+    op = cases.gpu_operator(p)
+    lv = cases.gpu_level(box, s)
+    ref = s.copy()
+    mi = 0.0
+    for _ in range(2):
+        dt_ref = O.stable_dt(p, box, ref, 0.25, t)
+        dt, mi, _ = op.advance_rk4_cfl(lv, 0.25, time=t, max_inverse_dt=mi)
+        assert abs(dt - dt_ref) <= 1e-12 * dt_ref
+        O.advance_rk4(p, box, ref, t, dt_ref)
+        t += dt_ref
+    assert abs(mi - O.max_inverse_dt(p, box, ref, t)) <= 1e-12 * mi
+    got = lv.interior(slice(0, 5)).cpu().numpy()
+    want = O.interior(box, ref)
+    err = cases.rel_err(got - O.interior(box, s), want - O.interior(box, s))
+    assert np.all(err <= 1e-11), err
+
+
 def test_ks_disk_golden_on_gpu(G):
     """The Kerr-Schild disk example (40 SSPRK2 steps) on the GPU reproduces
     the reference's recorded disk mass (GRHD_PROGRESS.md:396-409)."""
