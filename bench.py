@@ -40,9 +40,10 @@ BYTES_PER_RHS_CELL = 80       # one RHS: 5 doubles read + 5 written
 METRIC = "GRHD cell-updates/s (RK4 step, KS torus a=0.9, 256^3, FP64)"
 
 
-def workload_config(n):
+def workload_config(n, precision="fp64"):
     return {
-        "workload": f"kerr_schild_torus_a0.9_{n}^3_rk4_fp64",
+        "workload": f"kerr_schild_torus_a0.9_{n}^3_rk4_{precision}",
+        "precision": precision,
         "grid": [n, n, n], "domain": [-HALF_WIDTH, HALF_WIDTH],
         "background": "KerrSchild M=1 a=0.9", "eos_gamma": GAMMA,
         "torus": {"inner_radius": 6.0, "pressure_max_radius": 12.0,
@@ -59,13 +60,14 @@ def workload_config(n):
 # ----------------------------------------------------------------- GPU arm
 
 
-def make_operator(G, n):
+def make_operator(G, n, precision="fp64"):
     dx = 2.0 * HALF_WIDTH / n
     c = 0.5 * n * dx
     return G.TimeDependentFixedBGLevelDataFiniteVolumeOperator(
         G.IdealGasEOS(GAMMA), G.KerrSchild(mass=1.0, spin=SPIN, dx=dx), dx,
         (c, c, c), G.AtmosphereOptions(1e-10, 1e-12, 0.8), 2.0, True,
-        G.RecoveryOptions(80, 1e-12, 1e-12, 0.8), True, False, 1e-3, 1.5)
+        G.RecoveryOptions(80, 1e-12, 1e-12, 0.8), True, False, 1e-3, 1.5,
+        precision=precision)
 
 
 def build_state(G, op, n, device):
@@ -147,7 +149,7 @@ def run_ours(args, rank, world, local_rank):
     device = f"cuda:{local_rank}"
     torch.cuda.set_device(local_rank)
     n = args.n
-    op = make_operator(G, n)
+    op = make_operator(G, n, args.precision)
     lv = build_state(G, op, n, device)
     cells = lv.num_cells
     dist = world > 1
@@ -351,6 +353,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=N_CELLS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", choices=["fp64", "mixed"],
+                    default="fp64")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -409,10 +413,11 @@ def main():
             "warmup": args.warmup,
             "ms_per_step": res["ms"] / args.steps,
             "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic (seeded torus initial data generated on the "
                     "device)",
-            "config": dict(workload_config(args.n),
+            "config": dict(workload_config(args.n, args.precision),
                            parallelism=f"replicas x{world}"),
             "e2e": res["e2e"], "roofline": res["roofline"],
             "cpu_baseline": cpu, "clocks": res["clocks"],

@@ -21,6 +21,9 @@ GRHD_ERR_SETUP = 4
 GRHD_BG_KERR_SCHILD = 0
 GRHD_BG_BINARY_PN = 1
 
+GRHD_PRECISION_FP64 = 0
+GRHD_PRECISION_MIXED = 1
+
 NUM_STATE_COMPS = 11
 NUM_CONSERVED = 5
 
@@ -49,6 +52,8 @@ class Params(C.Structure):
         ("use_metric_volume_time_sources", C.c_int),
         ("metric_time_derivative_step", C.c_double),
         ("excision_radius", C.c_double),
+        ("accretion_radius", C.c_double),
+        ("precision", C.c_int),
     ]
 
 
@@ -143,6 +148,7 @@ SIGNATURES = {
     "grhd_profile_enable": (C.c_int, [_vp, C.c_int]),
     "grhd_profile_read": (C.c_int, [_vp, _P(C.c_double), _P(C.c_longlong)]),
     "grhd_launch_count": (C.c_longlong, [_vp]),
+    "grhd_accretion": (C.c_int, [_vp, _dp, _dp, C.c_int]),
 }
 
 _lib = None

@@ -29,6 +29,9 @@ struct grhd_ctx
     size_t int_cap = 0;      // doubles per interior buffer
     double *stage = nullptr; // 11 comps over the ghosted box
     size_t stage_cap = 0;
+    double *mdot_part = nullptr; // per face-kernel block accretion sums
+    size_t mdot_cap = 0;
+    double *mdot_acc = nullptr;  // [Mdot of the last RHS, time integral]
     DevStatus *status = nullptr;   // device
     DevStatus *status_h = nullptr; // pinned host mirror
     double *probe = nullptr;       // device scalars: probe + torus setup
@@ -139,6 +142,7 @@ Options make_options(const grhd_params &p)
     o.use_src = p.use_static_metric_sources;
     o.use_vol = p.use_metric_volume_time_sources;
     o.excision_radius = p.excision_radius;
+    o.accretion_radius = p.accretion_radius;
     o.dx = p.dx;
     for (int d = 0; d < 3; ++d)
         o.center[d] = p.center[d];
@@ -269,9 +273,13 @@ int ensure_scratch(grhd_ctx *ctx, const BoxDev &b, bool need_stage)
             return st;
         ctx->int_cap = ni;
     }
-    if (need_stage)
-        st = grow(ctx, &ctx->stage, &ctx->stage_cap,
-                  kStateComps * (size_t)b.gvol());
+    if (need_stage &&
+        (st = grow(ctx, &ctx->stage, &ctx->stage_cap,
+                   kStateComps * (size_t)b.gvol())))
+        return st;
+    if (ctx->params.accretion_radius > 0.0)
+        st = grow(ctx, &ctx->mdot_part, &ctx->mdot_cap,
+                  (size_t)face_kernel_blocks(b, ctx->zchunk));
     return st;
 }
 
@@ -365,24 +373,37 @@ void read_diag(const grhd_ctx *ctx, grhd_diagnostics *d)
 // One RHS evaluation on the device (no synchronisation).  With
 // `prepared` the interior primitive cache and sources were already
 // written by the previous fused stage kernel for this state and time.
-void enqueue_rhs(grhd_ctx *ctx, double *rhs, double *state, const BoxDev &b,
+// `mdot_weight` is the weight of this RHS's accretion rate in the time
+// integral (the stage weight times dt).
+// The scratch buffers are allocated in doubles; the mixed path (T = float)
+// uses their first half.
+template <typename T> T *scratch(double *p) { return reinterpret_cast<T *>(p); }
+
+template <typename T>
+void enqueue_rhs(grhd_ctx *ctx, T *rhs, double *state, const BoxDev &b,
                  const Background &bg, const double inv_dx[3], cudaStream_t s,
-                 bool prepared = false)
+                 bool prepared = false, double mdot_weight = 0.0)
 {
+    T *prim = scratch<T>(ctx->prim), *src = scratch<T>(ctx->src);
     {
         Timed t_(ctx, GRHD_K_GHOSTS, s);
-        launch_fill_ghosts(state, ctx->prim, b, bg, ctx->opt, ctx->status, s);
+        launch_fill_ghosts<T>(state, prim, b, bg, ctx->opt, ctx->status, s);
     }
     if (!prepared)
     {
         Timed t_(ctx, GRHD_K_CELLS, s);
-        launch_cells(state, ctx->prim, ctx->src, b, bg, ctx->opt, ctx->status,
-                     s);
+        launch_cells<T>(state, prim, src, b, bg, ctx->opt, ctx->status, s);
     }
     {
         Timed t_(ctx, GRHD_K_FACES, s);
-        launch_faces(ctx->prim, ctx->src, rhs, b, bg, ctx->opt, inv_dx,
-                     ctx->zchunk, s);
+        launch_faces<T>(prim, src, rhs, b, bg, ctx->opt, inv_dx, ctx->zchunk,
+                        ctx->mdot_part, s);
+    }
+    if (ctx->params.accretion_radius > 0.0)
+    {
+        ++ctx->launches;
+        launch_mdot_sum(ctx->mdot_part, face_kernel_blocks(b, ctx->zchunk),
+                        mdot_weight, ctx->mdot_acc, s);
     }
 }
 
@@ -445,6 +466,8 @@ void grhd_default_params(grhd_params *p)
     p->use_metric_volume_time_sources = 0;
     p->metric_time_derivative_step = 1.0e-3;
     p->excision_radius = 0.0;
+    p->accretion_radius = 0.0;
+    p->precision = GRHD_PRECISION_FP64;
 }
 
 const char *grhd_status_string(int status)
@@ -484,6 +507,9 @@ int grhd_create(const grhd_params *params, grhd_ctx **out)
     if (params->background != GRHD_BG_KERR_SCHILD &&
         params->background != GRHD_BG_BINARY_PN)
         return GRHD_ERR_INVALID_ARG;
+    if (params->precision != GRHD_PRECISION_FP64 &&
+        params->precision != GRHD_PRECISION_MIXED)
+        return GRHD_ERR_INVALID_ARG;
     grhd_ctx *ctx = new (std::nothrow) grhd_ctx();
     if (!ctx)
         return GRHD_ERR_SETUP;
@@ -496,7 +522,10 @@ int grhd_create(const grhd_params *params, grhd_ctx **out)
         cudaMallocHost((void **)&ctx->status_h, sizeof(DevStatus)) !=
             cudaSuccess ||
         cudaMalloc((void **)&ctx->probe, 8 * sizeof(double)) != cudaSuccess ||
-        cudaMalloc((void **)&ctx->flag, sizeof(int)) != cudaSuccess)
+        cudaMalloc((void **)&ctx->flag, sizeof(int)) != cudaSuccess ||
+        cudaMalloc((void **)&ctx->mdot_acc, 2 * sizeof(double)) !=
+            cudaSuccess ||
+        cudaMemset(ctx->mdot_acc, 0, 2 * sizeof(double)) != cudaSuccess)
     {
         grhd_destroy(ctx);
         return GRHD_ERR_CUDA;
@@ -517,6 +546,8 @@ void grhd_destroy(grhd_ctx *ctx)
     cudaFree(ctx->status);
     cudaFree(ctx->probe);
     cudaFree(ctx->flag);
+    cudaFree(ctx->mdot_part);
+    cudaFree(ctx->mdot_acc);
     if (ctx->status_h)
         cudaFreeHost(ctx->status_h);
     for (auto &r : ctx->prof_pending)
@@ -554,12 +585,20 @@ int grhd_compute_rhs(grhd_ctx *ctx, double *rhs, int64_t rhs_cs,
         return st;
     const Background bg = make_background(ctx->params, time);
     // the face kernel writes with the interior-volume stride; a caller
-    // stride that differs goes through the k scratch buffer
-    if (rhs_cs == b.ivol())
-        enqueue_rhs(ctx, rhs, state, b, bg, inverse_dx, s);
+    // stride that differs, or the mixed path's FP32 RHS, goes through the
+    // k scratch buffer
+    if (ctx->params.precision == GRHD_PRECISION_MIXED)
+    {
+        enqueue_rhs<float>(ctx, scratch<float>(ctx->kbuf), state, b, bg,
+                           inverse_dx, s);
+        ++ctx->launches;
+        launch_widen(scratch<float>(ctx->kbuf), b.ivol(), rhs, rhs_cs, s);
+    }
+    else if (rhs_cs == b.ivol())
+        enqueue_rhs<double>(ctx, rhs, state, b, bg, inverse_dx, s);
     else
     {
-        enqueue_rhs(ctx, ctx->kbuf, state, b, bg, inverse_dx, s);
+        enqueue_rhs<double>(ctx, ctx->kbuf, state, b, bg, inverse_dx, s);
         for (int c = 0; c < 5; ++c)
             GRHD_CUDA(ctx, cudaMemcpyAsync(rhs + c * rhs_cs,
                                            ctx->kbuf + c * b.ivol(),
@@ -671,86 +710,9 @@ int grhd_compute_stable_dt(grhd_ctx *ctx, const double *state,
     return GRHD_OK;
 }
 
-int grhd_advance_ssprk2(grhd_ctx *ctx, double *state, int64_t state_cs,
-                        const grhd_box *box, const double inverse_dx[3],
-                        double time, double dt, grhd_diagnostics *diag,
-                        void *stream)
-{
-    int st = common_checks(ctx, state, box);
-    if (st)
-        return st;
-    if (!inverse_dx || !box_is_domain(box))
-        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
-                         "advance needs the box to cover the whole domain");
-    cudaStream_t s = (cudaStream_t)stream;
-    const BoxDev b = make_box(box, state_cs);
-    if ((st = check_strides(ctx, b, state_cs, -1)) ||
-        (st = ensure_scratch(ctx, b, true)) || (st = reset_status(ctx, s)))
-        return st;
-    BoxDev sb = b; // the stage buffer is packed: stride = ghosted volume
-    sb.cs = b.gvol();
-    const Background bg0 = make_background(ctx->params, time);
-    const Background bg1 = make_background(ctx->params, time + dt);
-    // rhs_initial = L(state); stage = state + dt rhs_initial recovered at
-    // t + dt, fused with the primitive cache and sources of L(stage)
-    enqueue_rhs(ctx, ctx->kbuf, state, b, bg0, inverse_dx, s);
-    {
-        Timed t_(ctx, GRHD_K_STAGE, s);
-        launch_stage(1, state, b.cs, nullptr, 0, ctx->stage, sb.cs, ctx->kbuf,
-                     nullptr, ctx->prim, ctx->src, b, bg1, ctx->opt, 0, dt,
-                     false, inverse_dx, ctx->status, s);
-    }
-    // rhs_stage = L(stage) at t + dt, then the SSPRK2 combination
-    enqueue_rhs(ctx, ctx->kbuf, ctx->stage, sb, bg1, inverse_dx, s, true);
-    {
-        Timed t_(ctx, GRHD_K_STAGE, s);
-        launch_stage(2, state, b.cs, ctx->stage, sb.cs, state, b.cs,
-                     ctx->kbuf, nullptr, nullptr, nullptr, b, bg1, ctx->opt,
-                     0, dt, false, inverse_dx, ctx->status, s);
-    }
-    st = finish_status(ctx, b, state, bg0, s);
-    read_diag(ctx, diag);
-    return st;
-}
-
 } // extern "C"
 
 namespace {
-
-// Classic RK4 (new): stage RHS times t, t+dt/2, t+dt/2, t+dt; every stage
-// combination is fused with the post-update recovery at the next RHS time
-// and with that RHS's per-cell work; the last stage optionally computes the
-// next CFL speed.  No host synchronisation.
-void enqueue_rk4(grhd_ctx *ctx, double *state, const BoxDev &b,
-                 const double inverse_dx[3], double time, double dt,
-                 bool want_cfl, cudaStream_t s)
-{
-    BoxDev sb = b;
-    sb.cs = b.gvol();
-    const Background bgs[4] = {
-        make_background(ctx->params, time),
-        make_background(ctx->params, time + 0.5 * dt),
-        make_background(ctx->params, time + 0.5 * dt),
-        make_background(ctx->params, time + dt)};
-    for (int stage = 0; stage < 4; ++stage)
-    {
-        if (stage == 0)
-            enqueue_rhs(ctx, ctx->kbuf, state, b, bgs[0], inverse_dx, s);
-        else
-            enqueue_rhs(ctx, ctx->kbuf, ctx->stage, sb, bgs[stage],
-                        inverse_dx, s, true);
-        Timed t_(ctx, GRHD_K_STAGE, s);
-        if (stage < 3)
-            launch_stage(0, state, b.cs, nullptr, 0, ctx->stage, sb.cs,
-                         ctx->kbuf, ctx->acc, ctx->prim, ctx->src, b,
-                         bgs[stage + 1], ctx->opt, stage, dt, false,
-                         inverse_dx, ctx->status, s);
-        else
-            launch_stage(0, state, b.cs, nullptr, 0, state, b.cs, ctx->kbuf,
-                         ctx->acc, nullptr, nullptr, b, bgs[3], ctx->opt,
-                         stage, dt, want_cfl, inverse_dx, ctx->status, s);
-    }
-}
 
 int advance_checks(grhd_ctx *ctx, double *state, int64_t state_cs,
                    const grhd_box *box, const double inverse_dx[3],
@@ -776,9 +738,108 @@ double bits_to_double(unsigned long long bits)
     return v;
 }
 
+// advance_ssprk2 (:563-589 / :782-809): rhs_initial = L(state); stage =
+// state + dt rhs_initial recovered at t + dt, fused with the primitive
+// cache and sources of L(stage); then the SSPRK2 combination.
+template <typename T>
+void enqueue_ssprk2(grhd_ctx *ctx, double *state, const BoxDev &b,
+                    const double inverse_dx[3], double time, double dt,
+                    cudaStream_t s)
+{
+    BoxDev sb = b; // the stage buffer is packed: stride = ghosted volume
+    sb.cs = b.gvol();
+    const Background bg0 = make_background(ctx->params, time);
+    const Background bg1 = make_background(ctx->params, time + dt);
+    T *k = scratch<T>(ctx->kbuf), *prim = scratch<T>(ctx->prim),
+      *src = scratch<T>(ctx->src);
+    enqueue_rhs<T>(ctx, k, state, b, bg0, inverse_dx, s, false, 0.5 * dt);
+    {
+        Timed t_(ctx, GRHD_K_STAGE, s);
+        launch_stage<T>(1, state, b.cs, nullptr, 0, ctx->stage, sb.cs, k,
+                        nullptr, prim, src, true, b, bg1, ctx->opt, 0, dt,
+                        false, inverse_dx, ctx->status, s);
+    }
+    enqueue_rhs<T>(ctx, k, ctx->stage, sb, bg1, inverse_dx, s, true, 0.5 * dt);
+    {
+        Timed t_(ctx, GRHD_K_STAGE, s);
+        launch_stage<T>(2, state, b.cs, ctx->stage, sb.cs, state, b.cs, k,
+                        nullptr, prim, nullptr, false, b, bg1, ctx->opt, 0, dt,
+                        false, inverse_dx, ctx->status, s);
+    }
+}
+
+// Classic RK4 (new): stage RHS times t, t+dt/2, t+dt/2, t+dt; every stage
+// combination is fused with the post-update recovery at the next RHS time
+// and with that RHS's per-cell work; the last stage optionally computes the
+// next CFL speed.  No host synchronisation.
+template <typename T>
+void enqueue_rk4(grhd_ctx *ctx, double *state, const BoxDev &b,
+                 const double inverse_dx[3], double time, double dt,
+                 bool want_cfl, cudaStream_t s)
+{
+    BoxDev sb = b;
+    sb.cs = b.gvol();
+    const Background bgs[4] = {
+        make_background(ctx->params, time),
+        make_background(ctx->params, time + 0.5 * dt),
+        make_background(ctx->params, time + 0.5 * dt),
+        make_background(ctx->params, time + dt)};
+    T *k = scratch<T>(ctx->kbuf), *prim = scratch<T>(ctx->prim),
+      *src = scratch<T>(ctx->src);
+    for (int stage = 0; stage < 4; ++stage)
+    {
+        const double w = (dt / 6.0) * ((stage == 1 || stage == 2) ? 2.0 : 1.0);
+        if (stage == 0)
+            enqueue_rhs<T>(ctx, k, state, b, bgs[0], inverse_dx, s, false, w);
+        else
+            enqueue_rhs<T>(ctx, k, ctx->stage, sb, bgs[stage], inverse_dx, s,
+                           true, w);
+        Timed t_(ctx, GRHD_K_STAGE, s);
+        if (stage < 3)
+            launch_stage<T>(0, state, b.cs, nullptr, 0, ctx->stage, sb.cs, k,
+                            ctx->acc, prim, src, true, b, bgs[stage + 1],
+                            ctx->opt, stage, dt, false, inverse_dx,
+                            ctx->status, s);
+        else
+            launch_stage<T>(0, state, b.cs, nullptr, 0, state, b.cs, k,
+                            ctx->acc, prim, nullptr, false, b, bgs[3],
+                            ctx->opt, stage, dt, want_cfl, inverse_dx,
+                            ctx->status, s);
+    }
+}
+
+void enqueue_rk4_any(grhd_ctx *ctx, double *state, const BoxDev &b,
+                     const double inverse_dx[3], double time, double dt,
+                     bool want_cfl, cudaStream_t s)
+{
+    if (ctx->params.precision == GRHD_PRECISION_MIXED)
+        enqueue_rk4<float>(ctx, state, b, inverse_dx, time, dt, want_cfl, s);
+    else
+        enqueue_rk4<double>(ctx, state, b, inverse_dx, time, dt, want_cfl, s);
+}
+
 } // namespace
 
 extern "C" {
+
+int grhd_advance_ssprk2(grhd_ctx *ctx, double *state, int64_t state_cs,
+                        const grhd_box *box, const double inverse_dx[3],
+                        double time, double dt, grhd_diagnostics *diag,
+                        void *stream)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    BoxDev b;
+    int st = advance_checks(ctx, state, state_cs, box, inverse_dx, b, s);
+    if (st)
+        return st;
+    if (ctx->params.precision == GRHD_PRECISION_MIXED)
+        enqueue_ssprk2<float>(ctx, state, b, inverse_dx, time, dt, s);
+    else
+        enqueue_ssprk2<double>(ctx, state, b, inverse_dx, time, dt, s);
+    st = finish_status(ctx, b, state, make_background(ctx->params, time), s);
+    read_diag(ctx, diag);
+    return st;
+}
 
 int grhd_advance_rk4(grhd_ctx *ctx, double *state, int64_t state_cs,
                      const grhd_box *box, const double inverse_dx[3],
@@ -790,7 +851,7 @@ int grhd_advance_rk4(grhd_ctx *ctx, double *state, int64_t state_cs,
     int st = advance_checks(ctx, state, state_cs, box, inverse_dx, b, s);
     if (st)
         return st;
-    enqueue_rk4(ctx, state, b, inverse_dx, time, dt, false, s);
+    enqueue_rk4_any(ctx, state, b, inverse_dx, time, dt, false, s);
     st = finish_status(ctx, b, state, make_background(ctx->params, time), s);
     read_diag(ctx, diag);
     return st;
@@ -831,7 +892,7 @@ int grhd_advance_rk4_cfl(grhd_ctx *ctx, double *state, int64_t state_cs,
     double dt = cfl / std::fmax(mi, 1.0e-14);
     if (max_dt > 0.0)
         dt = std::fmin(dt, max_dt);
-    enqueue_rk4(ctx, state, b, inverse_dx, time, dt, true, s);
+    enqueue_rk4_any(ctx, state, b, inverse_dx, time, dt, true, s);
     st = finish_status(ctx, b, state, bg0, s);
     read_diag(ctx, diag);
     if (st)
@@ -1011,6 +1072,24 @@ int grhd_profile_read(grhd_ctx *ctx, double ms[GRHD_K_NUM_CLASSES],
         ctx->event_pool.push_back(r.b);
     }
     ctx->prof_pending.clear();
+    return GRHD_OK;
+}
+
+int grhd_accretion(grhd_ctx *ctx, double *mdot_last, double *integral,
+                   int reset)
+{
+    if (!ctx)
+        return GRHD_ERR_INVALID_ARG;
+    double h[2];
+    GRHD_CUDA(ctx, cudaSetDevice(ctx->device));
+    GRHD_CUDA(ctx, cudaMemcpy(h, ctx->mdot_acc, 2 * sizeof(double),
+                              cudaMemcpyDeviceToHost));
+    if (mdot_last)
+        *mdot_last = h[0];
+    if (integral)
+        *integral = h[1];
+    if (reset)
+        GRHD_CUDA(ctx, cudaMemset(ctx->mdot_acc + 1, 0, sizeof(double)));
     return GRHD_OK;
 }
 

@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(128)
         cell_xyz(o, i, j, kk, x, y, z);
         const double radius = sqrt(x * x + y * y + z * z);
         Geo g;
-        ks_metric<false>(c.mass, 0.0, x, y, z, g, nullptr);
+        ks_metric<double, false>(c.mass, 0.0, x, y, z, g, nullptr);
         Prim pr;
         if (radius < c.atmosphere_radius)
             pr = atmosphere(o);
@@ -397,7 +397,7 @@ __global__ void __launch_bounds__(128)
             const double rho = ok ? mi_density(c, k, radius, ok) : 0.0;
             // Michel velocity on the +x axis in Kerr-Schild coordinates
             Geo ga;
-            ks_metric<false>(c.mass, 0.0, radius, 0.0, 0.0, ga, nullptr);
+            ks_metric<double, false>(c.mass, 0.0, radius, 0.0, 0.0, ga, nullptr);
             double W = 0.0, vr = 0.0;
             if (ok)
             {

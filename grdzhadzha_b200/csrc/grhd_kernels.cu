@@ -1,20 +1,27 @@
 // grhd_kernels.cu -- sm_100a kernels of the fixed-background Valencia GRHD
-// operator (FP64).
+// operator.
+//
+// The kernels are templated on the arithmetic type T of the primitive
+// cache, the face fluxes, the sources and the RHS: T = double is the FP64
+// path, T = float the mixed path (the conserved state, the RK accumulator
+// and con2prim stay FP64 in both).
 //
 // One RHS evaluation is three launches:
 //   fill_ghosts : physical (outflow) ghost cells of the box, as
 //                 fill_conserved_outflow_boundaries_from_fixed_background
-//                 (FixedBGFArrayBoxFiniteVolume.hpp:113-177);
-//   cells       : per cell of the ghosted box, metric + con2prim into the
-//                 primitive scratch (recover_primitives_from_fixed_background,
-//                 :33-58), and for interior cells the static-metric and
-//                 volume-time sources (:255-298, :616-675);
-//   faces       : every face of the box computed once -- MUSCL slopes,
-//                 floors, p2c, HLLE -- with the flux divergence and the
-//                 sources written straight to the RHS (:179-253, :300-363).
-// The reference evaluates each face twice and every direction in a
-// separate pass over the box; here each face is evaluated once and the
-// interface states never leave registers / shared memory.
+//                 (FixedBGFArrayBoxFiniteVolume.hpp:113-177), then the
+//                 ghost cells' con2prim into the primitive cache;
+//   cells       : interior cells: metric + con2prim into the primitive
+//                 cache (recover_primitives_from_fixed_background, :33-58)
+//                 and the static-metric and volume-time sources (:255-298,
+//                 :616-675);
+//   faces       : the face fluxes -- MUSCL slopes, floors, p2c, HLLE --
+//                 with the flux divergence and the sources written straight
+//                 to the RHS (:179-253, :300-363).
+// Inside the RK integrators the per-cell work of the next RHS is fused into
+// the stage kernel, so `cells` runs once per step.  The reference evaluates
+// every face twice and every direction in a separate pass over the box;
+// here the interface states never leave registers / shared memory.
 #include "grhd_kernels.cuh"
 
 namespace grhd {
@@ -83,6 +90,59 @@ __device__ __forceinline__ bool primitive_differs(const Prim &a, const Prim &b)
            a.v[0] != b.v[0] || a.v[1] != b.v[1] || a.v[2] != b.v[2];
 }
 
+template <typename T>
+__device__ __forceinline__ void store_pv(T *prim, int64_t pcs, int64_t g,
+                                         const Prim &pr)
+{
+    prim[0 * pcs + g] = T(pr.rho);
+    prim[1 * pcs + g] = T(pr.p);
+    prim[2 * pcs + g] = T(pr.v[0]);
+    prim[3 * pcs + g] = T(pr.v[1]);
+    prim[4 * pcs + g] = T(pr.v[2]);
+}
+
+template <typename T>
+__device__ __forceinline__ void store_src(T *src, int64_t rcs, int64_t ri,
+                                          const ConsT<T> &s)
+{
+    src[0 * rcs + ri] = s.D;
+    src[1 * rcs + ri] = s.S[0];
+    src[2 * rcs + ri] = s.S[1];
+    src[3 * rcs + ri] = s.S[2];
+    src[4 * rcs + ri] = s.tau;
+}
+
+template <typename T> __device__ __forceinline__ ConsT<T> zero_cons()
+{
+    ConsT<T> z;
+    z.D = z.tau = z.S[0] = z.S[1] = z.S[2] = T(0);
+    return z;
+}
+
+// con2prim of a cell: the reference's bracketed solve (FP64 path) or the
+// warm-started FP64 solve from a nearby pressure (mixed path).
+template <typename T>
+__device__ __forceinline__ bool cell_con2prim(const Options &o, const Cons &c,
+                                              const GeoT<T> &g, double p_guess,
+                                              Prim &out)
+{
+    double gUU[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+        gUU[q] = double(g.gUU[q]);
+    if (sizeof(T) == sizeof(double))
+        return con2prim(o, c, gUU, out, nullptr, nullptr);
+    return con2prim_warm(o, c, gUU, p_guess, out);
+}
+
+template <typename T>
+__device__ __forceinline__ void gLL_double(const GeoT<T> &g, double out[6])
+{
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+        out[q] = double(g.gLL[q]);
+}
+
 // ------------------------------------------------------------ ghost fill
 
 // Enumerates the shell "ghosted box minus interior box" as three slabs:
@@ -133,24 +193,15 @@ __device__ __forceinline__ bool shell_cell(const BoxDev &b, int64_t t, int &i,
     return false;
 }
 
-__device__ __forceinline__ void store_pv(double *prim, int64_t pcs,
-                                         int64_t g, const Prim &pr)
-{
-    prim[0 * pcs + g] = pr.rho;
-    prim[1 * pcs + g] = pr.p;
-    prim[2 * pcs + g] = pr.v[0];
-    prim[3 * pcs + g] = pr.v[1];
-    prim[4 * pcs + g] = pr.v[2];
-}
-
 // Physical (outflow) ghost fill of the shell "ghosted box minus box"
 // (fill_conserved_outflow_boundaries_from_fixed_background, :113-177),
 // then, for every shell cell, the ghosted-box con2prim of the RHS into the
-// primitive cache (recover_primitives_from_fixed_background, :33-58).
+// primitive cache (recover_primitives_from_fixed_background, :33-58).  The
+// fill itself is FP64 in both paths.
+template <typename T>
 __global__ void __launch_bounds__(256)
-    k_fill_ghosts(double *__restrict__ state, double *__restrict__ prim,
-                  BoxDev b, Background bg, Options o, DevStatus *st,
-                  int64_t nshell)
+    k_fill_ghosts(double *__restrict__ state, T *__restrict__ prim, BoxDev b,
+                  Background bg, Options o, DevStatus *st, int64_t nshell)
 {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
          t < nshell; t += (int64_t)gridDim.x * blockDim.x)
@@ -214,22 +265,22 @@ __global__ void __launch_bounds__(256)
 }
 
 // Static-metric sources (:255-298) from the floored primitives and, for
-// the binary, the volume-time source (:616-675); `pr` is the cell's
-// unfloored con2prim result.
-__device__ __forceinline__ Cons cell_sources(const Options &o,
-                                             const Background &bg, double x,
-                                             double y, double z,
-                                             const Prim &pr, const Cons &c,
-                                             const GeoFull &f)
+// the binary, the volume-time source (:616-675, FP64 in both paths); `pr`
+// is the cell's unfloored con2prim result.
+template <typename T>
+__device__ __forceinline__ ConsT<T> cell_sources(const Options &o,
+                                                 const Background &bg,
+                                                 double x, double y, double z,
+                                                 const Prim &pr, const Cons &c,
+                                                 const GeoFullT<T> &f)
 {
-    Cons s;
-    s.D = s.tau = s.S[0] = s.S[1] = s.S[2] = 0.0;
+    ConsT<T> s = zero_cons<T>();
     if (o.use_src)
     {
-        Prim fp = pr;
+        PrimT<T> fp = convert_prim<double, T>(pr);
         floors(o, fp, f.g.gLL);
         if (!is_atmo(o, fp, o.src_atmo_factor))
-            s = static_sources(fp, c, f);
+            s = static_sources(fp, convert_cons<double, T>(c), f);
     }
     if (o.use_vol && bg.kind == 1)
     {
@@ -240,23 +291,13 @@ __device__ __forceinline__ Cons cell_sources(const Options &o,
             __dadd_rn(pn_log_sqrt_det(__dadd_rn(1.0, 2.0 * Up)),
                       -pn_log_sqrt_det(__dadd_rn(1.0, 2.0 * Um))) /
             (2.0 * bg.fd_h);
-        s.D += 0.0 - c.D * dl;
-        s.tau += 0.0 - c.tau * dl;
+        s.D = T(double(s.D) + (0.0 - c.D * dl));
+        s.tau = T(double(s.tau) + (0.0 - c.tau * dl));
 #pragma unroll
         for (int m = 0; m < 3; ++m)
-            s.S[m] += 0.0 - c.S[m] * dl;
+            s.S[m] = T(double(s.S[m]) + (0.0 - c.S[m] * dl));
     }
     return s;
-}
-
-__device__ __forceinline__ void store_src(double *src, int64_t rcs,
-                                          int64_t ri, const Cons &s)
-{
-    src[0 * rcs + ri] = s.D;
-    src[1 * rcs + ri] = s.S[0];
-    src[2 * rcs + ri] = s.S[1];
-    src[3 * rcs + ri] = s.S[2];
-    src[4 * rcs + ri] = s.tau;
 }
 
 // ------------------------------------------------------- per-cell pass
@@ -264,10 +305,12 @@ __device__ __forceinline__ void store_src(double *src, int64_t rcs,
 // Interior cells: con2prim into the primitive cache (the ghosted-box
 // recovery of the RHS restricted to the interior; the shell is done by
 // k_fill_ghosts) and the sources into the source scratch.  Excised cells
-// keep their frozen primitives and get no source.
+// keep their frozen primitives and get no source.  The mixed path starts
+// con2prim from the state's stored pressure.
+template <typename T>
 __global__ void __launch_bounds__(256, 2)
-    k_cells(const double *__restrict__ state, double *__restrict__ prim,
-            double *__restrict__ src, BoxDev b, Background bg, Options o,
+    k_cells(const double *__restrict__ state, T *__restrict__ prim,
+            T *__restrict__ src, BoxDev b, Background bg, Options o,
             DevStatus *st)
 {
     const int64_t n = b.ivol();
@@ -279,8 +322,7 @@ __global__ void __launch_bounds__(256, 2)
         const int j = b.lo[1] + (int)(r % b.in[1]);
         const int k = b.lo[2] + (int)(r / b.in[1]);
         const int64_t g = b.gidx(i, j, k);
-        Cons s;
-        s.D = s.tau = s.S[0] = s.S[1] = s.S[2] = 0.0;
+        ConsT<T> s = zero_cons<T>();
         if (excised(o, i, j, k))
         {
             store_pv(prim, b.pcs, g, load_prim(state, b.cs, g));
@@ -289,14 +331,14 @@ __global__ void __launch_bounds__(256, 2)
         }
         double x, y, z;
         cell_xyz(o, i, j, k, x, y, z);
-        GeoFull f;
+        GeoFullT<T> f;
         if (o.use_src)
-            background_metric<true>(bg, x, y, z, f.g, &f);
+            metric_T<T, true>(bg, x, y, z, f.g, &f);
         else
-            background_metric<false>(bg, x, y, z, f.g, nullptr);
+            metric_T<T, false>(bg, x, y, z, f.g, nullptr);
         const Cons c = load_cons(state, b.cs, g);
         Prim pr;
-        if (!con2prim(o, c, f.g.gUU, pr, nullptr, nullptr))
+        if (!cell_con2prim(o, c, f.g, state[kPress * b.cs + g], pr))
         {
             record_error(st, 2, g);
             pr.rho = pr.p = 1.0;
@@ -304,7 +346,7 @@ __global__ void __launch_bounds__(256, 2)
             pr.eps = 1.0;
         }
         else
-            s = cell_sources(o, bg, x, y, z, pr, c, f);
+            s = cell_sources<T>(o, bg, x, y, z, pr, c, f);
         store_pv(prim, b.pcs, g, pr);
         store_src(src, b.rcs, t, s);
     }
@@ -312,8 +354,9 @@ __global__ void __launch_bounds__(256, 2)
 
 // ----------------------------------------------------------- face pass
 
-__device__ __forceinline__ void geo_store(double *g, int n, int cell,
-                                          const Geo &v)
+template <typename T>
+__device__ __forceinline__ void geo_store(T *g, int n, int cell,
+                                          const GeoT<T> &v)
 {
 #pragma unroll
     for (int s = 0; s < 6; ++s)
@@ -327,8 +370,9 @@ __device__ __forceinline__ void geo_store(double *g, int n, int cell,
         g[(13 + i) * n + cell] = v.shift[i];
 }
 
-__device__ __forceinline__ void geo_load(const double *g, int n, int cell,
-                                         Geo &v)
+template <typename T>
+__device__ __forceinline__ void geo_load(const T *g, int n, int cell,
+                                         GeoT<T> &v)
 {
 #pragma unroll
     for (int s = 0; s < 6; ++s)
@@ -342,35 +386,38 @@ __device__ __forceinline__ void geo_load(const double *g, int n, int cell,
         v.shift[i] = g[(13 + i) * n + cell];
 }
 
-__device__ __forceinline__ void geo_avg_smem(const double *g, int n, int ca,
-                                             int cb, Geo &v)
+template <typename T>
+__device__ __forceinline__ void geo_avg_smem(const T *g, int n, int ca, int cb,
+                                             GeoT<T> &v)
 {
 #pragma unroll
     for (int s = 0; s < 6; ++s)
     {
-        v.gLL[s] = 0.5 * (g[s * n + ca] + g[s * n + cb]);
-        v.gUU[s] = 0.5 * (g[(6 + s) * n + ca] + g[(6 + s) * n + cb]);
+        v.gLL[s] = T(0.5) * (g[s * n + ca] + g[s * n + cb]);
+        v.gUU[s] = T(0.5) * (g[(6 + s) * n + ca] + g[(6 + s) * n + cb]);
     }
-    v.lapse = 0.5 * (g[12 * n + ca] + g[12 * n + cb]);
+    v.lapse = T(0.5) * (g[12 * n + ca] + g[12 * n + cb]);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
-        v.shift[i] = 0.5 * (g[(13 + i) * n + ca] + g[(13 + i) * n + cb]);
+        v.shift[i] = T(0.5) * (g[(13 + i) * n + ca] + g[(13 + i) * n + cb]);
 }
 
-__device__ __forceinline__ PV load_pv_global(const double *__restrict__ prim,
-                                             int64_t pcs, int64_t idx)
+template <typename T>
+__device__ __forceinline__ PVT<T> load_pv_global(const T *__restrict__ prim,
+                                                 int64_t pcs, int64_t idx)
 {
-    PV p;
+    PVT<T> p;
 #pragma unroll
     for (int c = 0; c < 5; ++c)
         p.q[c] = __ldg(&prim[c * pcs + idx]);
     return p;
 }
 
-__device__ __forceinline__ PV load_pv_smem(const double *P, int cell)
+template <typename T>
+__device__ __forceinline__ PVT<T> load_pv_smem(const T *P, int cell)
 {
     constexpr int n = kPW * kPW;
-    PV p;
+    PVT<T> p;
 #pragma unroll
     for (int c = 0; c < 5; ++c)
         p.q[c] = P[c * n + cell];
@@ -378,7 +425,8 @@ __device__ __forceinline__ PV load_pv_smem(const double *P, int cell)
 }
 
 // Geometry of the cross-shaped (x,y) neighbourhood of a tile at plane kk.
-__device__ __forceinline__ void tile_geometry(double *G, const Background &bg,
+template <typename T>
+__device__ __forceinline__ void tile_geometry(T *G, const Background &bg,
                                               const Options &o, int i0,
                                               int j0, int kk, int tid)
 {
@@ -390,25 +438,80 @@ __device__ __forceinline__ void tile_geometry(double *G, const Background &bg,
             continue;
         double x, y, z;
         cell_xyz(o, i0 - 1 + u, j0 - 1 + v, kk, x, y, z);
-        Geo g;
-        background_metric<false>(bg, x, y, z, g, nullptr);
+        GeoT<T> g;
+        metric_T<T, false>(bg, x, y, z, g, nullptr);
         geo_store(G, n, idx, g);
     }
 }
 
-__global__ void __launch_bounds__(kTB *kTB, 2)
-    k_faces(const double *__restrict__ prim, const double *__restrict__ src,
-            double *__restrict__ rhs, BoxDev b, Background bg, Options o,
-            double idx0, double idx1, double idx2, int zchunk)
+// Rest-mass flux of one face through the voxelised sphere r < R (new):
+// the face between cells L and R (R = L + e_d) lies on the sphere's
+// boundary when exactly one of them is inside; the outward flux is
+// +sqrt(gamma_face) F_D dA when L is inside, and Mdot counts the inward
+// flux.
+template <typename T>
+__device__ __forceinline__ double mdot_face(const Options &o, int il, int jl,
+                                            int kl, int d, const GeoT<T> &gf,
+                                            T FD)
 {
-    extern __shared__ double smem[];
+    double x, y, z;
+    cell_xyz(o, il, jl, kl, x, y, z);
+    const bool in_l = sqrt(x * x + y * y + z * z) < o.accretion_radius;
+    cell_xyz(o, il + (d == 0), jl + (d == 1), kl + (d == 2), x, y, z);
+    const bool in_r = sqrt(x * x + y * y + z * z) < o.accretion_radius;
+    if (in_l == in_r)
+        return 0.0;
+    double g[6];
+    gLL_double(gf, g);
+    const double det = g[0] * (g[3] * g[5] - g[4] * g[4]) -
+                       g[1] * (g[1] * g[5] - g[4] * g[2]) +
+                       g[2] * (g[1] * g[4] - g[3] * g[2]);
+    return (in_l ? -1.0 : 1.0) * sqrt(det) * double(FD) * (o.dx * o.dx);
+}
+
+// Block sum of `v` into part[block] (fixed order within the block).
+__device__ __forceinline__ void block_partial(double v, double *scratch,
+                                              double *part, int tid, int nt,
+                                              int64_t block)
+{
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+        v += __shfl_down_sync(0xffffffffu, v, off);
+    if ((tid & 31) == 0)
+        scratch[tid >> 5] = v;
+    __syncthreads();
+    if (tid == 0)
+    {
+        double sum = 0.0;
+        for (int w = 0; w < nt / 32; ++w)
+            sum += scratch[w];
+        part[block] = sum;
+    }
+}
+
+// 16x16 threads own a 15x15 (x,y) cell tile and march along z over a chunk
+// of planes.  Per plane: the primitive cross tile (2-cell halo) and the
+// geometry cross tile (1-cell halo) in shared memory, geometry double
+// buffered by plane; x and y faces from shared memory (each tile also
+// evaluates its two boundary faces per row), the z face from a 4-plane
+// register window (each z face once); divergence + sources to the RHS.
+template <typename T, bool MDOT>
+__global__ void __launch_bounds__(kTB *kTB, 2)
+    k_faces(const T *__restrict__ prim, const T *__restrict__ src,
+            T *__restrict__ rhs, BoxDev b, Background bg, Options o,
+            double idx0_, double idx1_, double idx2_, int zchunk,
+            double *__restrict__ mdot_part)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *smem = reinterpret_cast<T *>(smem_raw);
     constexpr int nP = kPW * kPW;
     constexpr int nG = kGW * kGW;
     constexpr int nFx = kTB * kTC; // x faces: a in [0,16), b in [0,15)
-    double *P = smem;                       // [5][nP]
-    double *Gb = P + 5 * nP;                // [2][16][nG]
-    double *Fx = Gb + 2 * kGeoFields * nG;  // [5][nFx]
-    double *Fy = Fx + 5 * nFx;              // [5][nFx]
+    T *P = smem;                       // [5][nP]
+    T *Gb = P + 5 * nP;                // [2][16][nG]
+    T *Fx = Gb + 2 * kGeoFields * nG;  // [5][nFx]
+    T *Fy = Fx + 5 * nFx;              // [5][nFx]
+    const T idx0 = T(idx0_), idx1 = T(idx1_), idx2 = T(idx2_);
 
     const int a = threadIdx.x, bb = threadIdx.y;
     const int tid = bb * kTB + a;
@@ -421,11 +524,10 @@ __global__ void __launch_bounds__(kTB *kTB, 2)
     const int ci_c = min(ci, b.hi[0]), cj_c = min(cj, b.hi[1]);
 
     // own-column z window P(k-1..k+2) and the z face below k0
-    PV w0, w1, w2, w3;
-    Cons Flo;
+    PVT<T> w0, w1, w2, w3;
+    ConsT<T> Flo = zero_cons<T>();
     tile_geometry(Gb, bg, o, i0, j0, k0, tid);
     __syncthreads();
-    Flo.D = Flo.tau = Flo.S[0] = Flo.S[1] = Flo.S[2] = 0.0;
     {
         w0 = load_pv_global(prim, b.pcs, b.gidx(ci_c, cj_c, k0 - 2));
         w1 = load_pv_global(prim, b.pcs, b.gidx(ci_c, cj_c, k0 - 1));
@@ -435,8 +537,8 @@ __global__ void __launch_bounds__(kTB *kTB, 2)
         {
             double x, y, z;
             cell_xyz(o, ci, cj, k0 - 1, x, y, z);
-            Geo gl, gr, gf;
-            background_metric<false>(bg, x, y, z, gl, nullptr);
+            GeoT<T> gl, gr, gf;
+            metric_T<T, false>(bg, x, y, z, gl, nullptr);
             geo_load(Gb, nG, (bb + 1) * kGW + (a + 1), gr);
             average_geo(gl, gr, gf);
             Flo = face_flux(o, w0, w1, w2, w3, gf, 2);
@@ -448,10 +550,11 @@ __global__ void __launch_bounds__(kTB *kTB, 2)
     }
 
     int cur = 0;
+    double macc = 0.0;
     for (int k = k0; k <= k1; ++k)
     {
-        double *Gc = Gb + cur * kGeoFields * nG;
-        double *Gn = Gb + (cur ^ 1) * kGeoFields * nG;
+        T *Gc = Gb + cur * kGeoFields * nG;
+        T *Gn = Gb + (cur ^ 1) * kGeoFields * nG;
         w3 = load_pv_global(prim, b.pcs, b.gidx(ci_c, cj_c, k + 2));
         // primitive cross tile at plane k (clamped to the ghosted box)
         for (int idx = tid; idx < nP; idx += kTB * kTB)
@@ -473,13 +576,15 @@ __global__ void __launch_bounds__(kTB *kTB, 2)
         if (bb < kTC && cj <= b.hi[1] && i0 + a - 1 <= b.hi[0])
         {
             const int row = (bb + 2) * kPW;
-            Geo gf;
+            GeoT<T> gf;
             geo_avg_smem(Gc, nG, (bb + 1) * kGW + a, (bb + 1) * kGW + a + 1, gf);
-            const Cons f = face_flux(o, load_pv_smem(P, row + a),
-                                     load_pv_smem(P, row + a + 1),
-                                     load_pv_smem(P, row + a + 2),
-                                     load_pv_smem(P, row + a + 3), gf, 0);
+            const ConsT<T> f = face_flux(o, load_pv_smem(P, row + a),
+                                         load_pv_smem(P, row + a + 1),
+                                         load_pv_smem(P, row + a + 2),
+                                         load_pv_smem(P, row + a + 3), gf, 0);
             const int fi = bb * kTB + a;
+            if (MDOT && a < kTC && i0 + a <= b.hi[0])
+                macc += mdot_face(o, i0 + a - 1, cj, k, 0, gf, f.D);
             Fx[0 * nFx + fi] = f.D;
             Fx[1 * nFx + fi] = f.S[0];
             Fx[2 * nFx + fi] = f.S[1];
@@ -489,15 +594,17 @@ __global__ void __launch_bounds__(kTB *kTB, 2)
         // y face between rows (j0+bb-1, j0+bb) in column i0+a
         if (a < kTC && ci <= b.hi[0] && j0 + bb - 1 <= b.hi[1])
         {
-            Geo gf;
+            GeoT<T> gf;
             geo_avg_smem(Gc, nG, bb * kGW + a + 1, (bb + 1) * kGW + a + 1, gf);
             const int col = a + 2;
-            const Cons f = face_flux(o, load_pv_smem(P, bb * kPW + col),
-                                     load_pv_smem(P, (bb + 1) * kPW + col),
-                                     load_pv_smem(P, (bb + 2) * kPW + col),
-                                     load_pv_smem(P, (bb + 3) * kPW + col), gf,
-                                     1);
+            const ConsT<T> f = face_flux(o, load_pv_smem(P, bb * kPW + col),
+                                         load_pv_smem(P, (bb + 1) * kPW + col),
+                                         load_pv_smem(P, (bb + 2) * kPW + col),
+                                         load_pv_smem(P, (bb + 3) * kPW + col),
+                                         gf, 1);
             const int fi = a * kTB + bb;
+            if (MDOT && bb < kTC && j0 + bb <= b.hi[1])
+                macc += mdot_face(o, ci, j0 + bb - 1, k, 1, gf, f.D);
             Fy[0 * nFx + fi] = f.D;
             Fy[1 * nFx + fi] = f.S[0];
             Fy[2 * nFx + fi] = f.S[1];
@@ -505,16 +612,17 @@ __global__ void __launch_bounds__(kTB *kTB, 2)
             Fy[4 * nFx + fi] = f.tau;
         }
         // z face at k+1/2 for this column
-        Cons Fhi;
+        ConsT<T> Fhi = zero_cons<T>();
         if (col_ok)
         {
-            Geo gf;
+            GeoT<T> gf, gA, gB;
             const int cell = (bb + 1) * kGW + a + 1;
-            Geo gA, gB;
             geo_load(Gc, nG, cell, gA);
             geo_load(Gn, nG, cell, gB);
             average_geo(gA, gB, gf);
             Fhi = face_flux(o, w0, w1, w2, w3, gf, 2);
+            if (MDOT && k < b.hi[2])
+                macc += mdot_face(o, ci, cj, k, 2, gf, Fhi.D);
         }
         __syncthreads();
 
@@ -523,22 +631,22 @@ __global__ void __launch_bounds__(kTB *kTB, 2)
             const int fxl = bb * kTB + a, fxh = bb * kTB + a + 1;
             const int fyl = a * kTB + bb, fyh = a * kTB + bb + 1;
             const int64_t ri = b.iidx(ci, cj, k);
-            double out[5];
-            const double fl[5] = {Flo.D, Flo.S[0], Flo.S[1], Flo.S[2], Flo.tau};
-            const double fh[5] = {Fhi.D, Fhi.S[0], Fhi.S[1], Fhi.S[2], Fhi.tau};
+            T out[5];
+            const T fl[5] = {Flo.D, Flo.S[0], Flo.S[1], Flo.S[2], Flo.tau};
+            const T fh[5] = {Fhi.D, Fhi.S[0], Fhi.S[1], Fhi.S[2], Fhi.tau};
 #pragma unroll
             for (int c = 0; c < 5; ++c)
             {
-                const double rx = -idx0 * (Fx[c * nFx + fxh] - Fx[c * nFx + fxl]);
-                const double ry = -idx1 * (Fy[c * nFx + fyh] - Fy[c * nFx + fyl]);
-                const double rz = -idx2 * (fh[c] - fl[c]);
+                const T rx = -idx0 * (Fx[c * nFx + fxh] - Fx[c * nFx + fxl]);
+                const T ry = -idx1 * (Fy[c * nFx + fyh] - Fy[c * nFx + fyl]);
+                const T rz = -idx2 * (fh[c] - fl[c]);
                 out[c] = ((rx + ry) + rz) + __ldg(&src[c * b.rcs + ri]);
             }
             if (excised(o, ci, cj, k))
             {
 #pragma unroll
                 for (int c = 0; c < 5; ++c)
-                    out[c] = 0.0;
+                    out[c] = T(0);
             }
 #pragma unroll
             for (int c = 0; c < 5; ++c)
@@ -550,6 +658,29 @@ __global__ void __launch_bounds__(kTB *kTB, 2)
         w2 = w3;
         cur ^= 1;
         __syncthreads();
+    }
+    if (MDOT)
+        block_partial(macc, reinterpret_cast<double *>(smem_raw), mdot_part,
+                      tid, kTB * kTB,
+                      blockIdx.x + (int64_t)gridDim.x *
+                                       (blockIdx.y + (int64_t)gridDim.y *
+                                                         blockIdx.z));
+}
+
+// Mdot of one RHS evaluation: the block partials summed in a fixed order;
+// acc[0] = Mdot, acc[1] += weight * Mdot (the time integral).
+__global__ void k_mdot_sum(const double *__restrict__ part, int64_t n,
+                           double weight, double *acc)
+{
+    __shared__ double w[32];
+    double v = 0.0;
+    for (int64_t q = threadIdx.x; q < n; q += blockDim.x)
+        v += part[q];
+    block_partial(v, w, w + 8, threadIdx.x, blockDim.x, 0);
+    if (threadIdx.x == 0)
+    {
+        acc[0] = w[8];
+        acc[1] += weight * w[8];
     }
 }
 
@@ -701,9 +832,10 @@ __global__ void __launch_bounds__(256)
 // Characteristic-speed CFL contribution of one cell, sum_d max|lambda|/dx_d
 // (compute_max_inverse_dt_from_fixed_background, :398-409) for floored
 // primitives that are not atmosphere.
+template <typename T>
 __device__ __forceinline__ double cell_inverse_dt(const Options &o,
-                                                  const Prim &fp,
-                                                  const Geo &g,
+                                                  const PrimT<T> &fp,
+                                                  const GeoT<T> &g,
                                                   const double inv[3])
 {
     double cell = 0.0;
@@ -712,9 +844,9 @@ __device__ __forceinline__ double cell_inverse_dt(const Options &o,
 #pragma unroll
         for (int d = 0; d < 3; ++d)
         {
-            double lo, hi;
+            T lo, hi;
             char_speeds(o, fp, g, d, lo, hi);
-            cell += fmax(fabs(lo), fabs(hi)) * inv[d];
+            cell += double(max_(abs_(lo), abs_(hi))) * inv[d];
         }
     }
     return cell;
@@ -743,15 +875,17 @@ __device__ __forceinline__ void flush_max(DevStatus *st, double v)
 // acc = k1 (+ 2 k2 + 2 k3), stage 3 out = U^n + dt/6 (acc + k4);
 // 1 Euler update out = U^n + dt k (advance_ssprk2 stage, :578);
 // 2 SSPRK2 combine out = (U^n + U^1 + dt k)/2 (FArrayBoxFiniteVolume.hpp:
-// 942-969).
-template <int MODE>
+// 942-969).  The stage input k, the primitive cache and the sources are of
+// type T; U, the accumulator and con2prim are FP64.  The mixed path starts
+// con2prim from the primitive cache's pressure of the same cell.
+template <int MODE, typename T>
 __global__ void __launch_bounds__(256, 2)
     k_stage(const double *un, int64_t ucs, const double *us, int64_t tcs,
-            double *out, int64_t ocs, const double *__restrict__ kv,
-            double *__restrict__ acc, double *__restrict__ prim,
-            double *__restrict__ src, BoxDev b, Background bg, Options o,
-            int stage, double dt, int cfl, double i0, double i1, double i2,
-            DevStatus *st)
+            double *out, int64_t ocs, const T *__restrict__ kv,
+            double *__restrict__ acc, T *__restrict__ prim,
+            T *__restrict__ src, BoxDev b, Background bg, Options o,
+            int stage, double dt, int prep_flag, int cfl, double i0,
+            double i1, double i2, DevStatus *st)
 {
     unsigned long long cnt[4] = {0, 0, 0, 0};
     const int64_t n = b.ivol();
@@ -759,7 +893,8 @@ __global__ void __launch_bounds__(256, 2)
     const double cst = (stage == 2) ? dt : 0.5 * dt;
     const double dt6 = dt / 6.0;
     const double inv[3] = {i0, i1, i2};
-    const bool prep = prim != nullptr;
+    const bool prep = prep_flag != 0 && prim != nullptr;
+    const bool mixed = sizeof(T) != sizeof(double);
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_pad;
          t += (int64_t)gridDim.x * blockDim.x)
     {
@@ -777,9 +912,7 @@ __global__ void __launch_bounds__(256, 2)
                 if (prep)
                 {
                     store_pv(prim, b.pcs, g, load_prim(un, ucs, g));
-                    Cons z0;
-                    z0.D = z0.tau = z0.S[0] = z0.S[1] = z0.S[2] = 0.0;
-                    store_src(src, b.rcs, t, z0);
+                    store_src(src, b.rcs, t, zero_cons<T>());
                 }
             }
             else
@@ -789,7 +922,7 @@ __global__ void __launch_bounds__(256, 2)
 #pragma unroll
                 for (int c = 0; c < 5; ++c)
                 {
-                    const double kk = kv[c * b.rcs + t];
+                    const double kk = double(kv[c * b.rcs + t]);
                     const double u0 = un[comp_of[c] * ucs + g];
                     if (MODE == 0)
                     {
@@ -817,21 +950,25 @@ __global__ void __launch_bounds__(256, 2)
                 c.tau = u[4];
                 double x, y, z;
                 cell_xyz(o, i, j, k, x, y, z);
-                GeoFull f;
+                GeoFullT<T> f;
                 if (prep && o.use_src)
-                    background_metric<true>(bg, x, y, z, f.g, &f);
+                    metric_T<T, true>(bg, x, y, z, f.g, &f);
                 else
-                    background_metric<false>(bg, x, y, z, f.g, nullptr);
+                    metric_T<T, false>(bg, x, y, z, f.g, nullptr);
+                double gLL[6];
+                gLL_double(f.g, gLL);
+                const double p_guess =
+                    (mixed && prim) ? double(prim[1 * b.pcs + g]) : 0.0;
                 // recovery with atmosphere (:60-110)
                 Prim pr;
-                const bool ok = con2prim(o, c, f.g.gUU, pr, nullptr, nullptr);
+                const bool ok = cell_con2prim(o, c, f.g, p_guess, pr);
                 bool reset = !ok;
                 Prim stored;
                 cnt[0] += 1;
                 if (ok)
                 {
                     stored = pr;
-                    floors(o, stored, f.g.gLL);
+                    floors(o, stored, gLL);
                     reset = primitive_differs(pr, stored);
                     if (reset)
                         cnt[2] += 1;
@@ -844,9 +981,12 @@ __global__ void __launch_bounds__(256, 2)
                 if (reset)
                 {
                     cnt[3] += 1;
-                    c = p2c(stored, f.g.gLL);
+                    c = p2c(stored, gLL);
                 }
-                store_prim(out, ocs, g, stored);
+                // the RK stage buffer (prep) carries conserved variables
+                // only: its primitive components are never read
+                if (!prep)
+                    store_prim(out, ocs, g, stored);
                 store_cons(out, ocs, g, c);
                 if (prep || cfl)
                 {
@@ -855,7 +995,7 @@ __global__ void __launch_bounds__(256, 2)
                     Prim pn = pr;
                     bool okn = ok;
                     if (reset)
-                        okn = con2prim(o, c, f.g.gUU, pn, nullptr, nullptr);
+                        okn = cell_con2prim(o, c, f.g, stored.p, pn);
                     if (!okn)
                     {
                         record_error(st, cfl && !prep ? 4 : 2,
@@ -867,15 +1007,14 @@ __global__ void __launch_bounds__(256, 2)
                     if (prep)
                     {
                         store_pv(prim, b.pcs, g, pn);
-                        Cons s;
-                        s.D = s.tau = s.S[0] = s.S[1] = s.S[2] = 0.0;
+                        ConsT<T> s = zero_cons<T>();
                         if (okn)
-                            s = cell_sources(o, bg, x, y, z, pn, c, f);
+                            s = cell_sources<T>(o, bg, x, y, z, pn, c, f);
                         store_src(src, b.rcs, t, s);
                     }
                     if (cfl && okn)
                     {
-                        Prim fp = pn;
+                        PrimT<T> fp = convert_prim<double, T>(pn);
                         floors(o, fp, f.g.gLL);
                         cell_inv = cell_inverse_dt(o, fp, f.g, inv);
                     }
@@ -942,6 +1081,18 @@ __global__ void k_residual_probe(const double *__restrict__ state, BoxDev b,
     con2prim(o, load_cons(state, b.cs, b.gidx(i, j, k)), g.gUU, pr, nullptr,
              &res);
     *out = res;
+}
+
+// float RHS of the mixed path into the caller's FP64 array
+__global__ void k_widen(const float *__restrict__ in, int64_t n, double *out,
+                        int64_t ocs)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+         t < 5 * n; t += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int64_t c = t / n, r = t - c * n;
+        out[c * ocs + r] = double(in[t]);
+    }
 }
 
 __global__ void k_eval_background(int64_t n, const double *__restrict__ xyz,
@@ -1022,52 +1173,87 @@ int grid_for(int64_t n, int threads)
     return (int)(blocks < 1 ? 1 : blocks);
 }
 
+template <typename T> size_t faces_smem()
+{
+    return sizeof(T) *
+           (5 * kPW * kPW + 2 * kGeoFields * kGW * kGW + 2 * 5 * kTB * kTC);
+}
+
 } // namespace
 
 cudaError_t configure_kernels()
 {
-    return cudaFuncSetAttribute(k_faces,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)face_kernel_smem_bytes());
+    cudaError_t e = cudaSuccess;
+    const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_faces<double, false>, attr,
+                                 (int)faces_smem<double>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_faces<double, true>, attr,
+                                 (int)faces_smem<double>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_faces<float, false>, attr,
+                                 (int)faces_smem<float>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_faces<float, true>, attr,
+                                 (int)faces_smem<float>());
+    return e;
 }
 
-size_t face_kernel_smem_bytes()
+int64_t face_kernel_blocks(const BoxDev &b, int zchunk)
 {
-    return sizeof(double) *
-           (5 * kPW * kPW + 2 * kGeoFields * kGW * kGW + 2 * 5 * kTB * kTC);
+    if (zchunk < 1)
+        zchunk = 1;
+    return (int64_t)((b.in[0] + kTC - 1) / kTC) * ((b.in[1] + kTC - 1) / kTC) *
+           ((b.in[2] + zchunk - 1) / zchunk);
 }
 
-void launch_fill_ghosts(double *state, double *prim, const BoxDev &b,
+template <typename T>
+void launch_fill_ghosts(double *state, T *prim, const BoxDev &b,
                         const Background &bg, const Options &o, DevStatus *st,
                         cudaStream_t s)
 {
     const int64_t nshell = b.gvol() - b.ivol();
     if (nshell <= 0)
         return;
-    k_fill_ghosts<<<grid_for(nshell, 256), 256, 0, s>>>(state, prim, b, bg, o,
-                                                       st, nshell);
+    k_fill_ghosts<T><<<grid_for(nshell, 256), 256, 0, s>>>(state, prim, b, bg,
+                                                          o, st, nshell);
 }
 
-void launch_cells(const double *state, double *prim, double *src,
-                  const BoxDev &b, const Background &bg, const Options &o,
-                  DevStatus *st, cudaStream_t s)
+template <typename T>
+void launch_cells(const double *state, T *prim, T *src, const BoxDev &b,
+                  const Background &bg, const Options &o, DevStatus *st,
+                  cudaStream_t s)
 {
-    k_cells<<<grid_for(b.ivol(), 256), 256, 0, s>>>(state, prim, src, b, bg,
-                                                    o, st);
+    k_cells<T><<<grid_for(b.ivol(), 256), 256, 0, s>>>(state, prim, src, b, bg,
+                                                       o, st);
 }
 
-void launch_faces(const double *prim, const double *src, double *rhs,
-                  const BoxDev &b, const Background &bg, const Options &o,
-                  const double inv_dx[3], int zchunk, cudaStream_t s)
+template <typename T>
+void launch_faces(const T *prim, const T *src, T *rhs, const BoxDev &b,
+                  const Background &bg, const Options &o,
+                  const double inv_dx[3], int zchunk, double *mdot_part,
+                  cudaStream_t s)
 {
-    const size_t smem = face_kernel_smem_bytes();
     if (zchunk < 1)
         zchunk = 1;
     dim3 grid((b.in[0] + kTC - 1) / kTC, (b.in[1] + kTC - 1) / kTC,
               (b.in[2] + zchunk - 1) / zchunk);
     dim3 block(kTB, kTB);
-    k_faces<<<grid, block, smem, s>>>(prim, src, rhs, b, bg, o, inv_dx[0],
-                                      inv_dx[1], inv_dx[2], zchunk);
+    if (o.accretion_radius > 0.0 && mdot_part)
+        k_faces<T, true><<<grid, block, faces_smem<T>(), s>>>(
+            prim, src, rhs, b, bg, o, inv_dx[0], inv_dx[1], inv_dx[2], zchunk,
+            mdot_part);
+    else
+        k_faces<T, false><<<grid, block, faces_smem<T>(), s>>>(
+            prim, src, rhs, b, bg, o, inv_dx[0], inv_dx[1], inv_dx[2], zchunk,
+            nullptr);
+}
+
+void launch_mdot_sum(const double *part, int64_t n, double weight,
+                     double *acc, cudaStream_t s)
+{
+    k_mdot_sum<<<1, 256, 0, s>>>(part, n, weight, acc);
 }
 
 void launch_update(double *dst, int64_t dcs, const double *src_state,
@@ -1085,9 +1271,10 @@ void launch_recover(double *state, const BoxDev &b, const Background &bg,
     k_recover<<<grid_for(b.ivol(), 256), 256, 0, s>>>(state, b, bg, o, st);
 }
 
+template <typename T>
 void launch_stage(int mode, const double *un, int64_t ucs, const double *us,
-                  int64_t tcs, double *out, int64_t ocs, const double *k,
-                  double *acc, double *prim, double *src, const BoxDev &b,
+                  int64_t tcs, double *out, int64_t ocs, const T *k,
+                  double *acc, T *prim, T *src, bool prep, const BoxDev &b,
                   const Background &bg, const Options &o, int stage,
                   double dt, bool cfl, const double inv_dx[3], DevStatus *st,
                   cudaStream_t s)
@@ -1095,18 +1282,19 @@ void launch_stage(int mode, const double *un, int64_t ucs, const double *us,
     const int grid = grid_for(b.ivol(), 256);
     const double i0 = inv_dx ? inv_dx[0] : 0.0, i1 = inv_dx ? inv_dx[1] : 0.0,
                  i2 = inv_dx ? inv_dx[2] : 0.0;
+    const int pf = prep ? 1 : 0, cf = cfl ? 1 : 0;
     if (mode == 0)
-        k_stage<0><<<grid, 256, 0, s>>>(un, ucs, us, tcs, out, ocs, k, acc,
-                                        prim, src, b, bg, o, stage, dt,
-                                        cfl ? 1 : 0, i0, i1, i2, st);
+        k_stage<0, T><<<grid, 256, 0, s>>>(un, ucs, us, tcs, out, ocs, k, acc,
+                                           prim, src, b, bg, o, stage, dt, pf,
+                                           cf, i0, i1, i2, st);
     else if (mode == 1)
-        k_stage<1><<<grid, 256, 0, s>>>(un, ucs, us, tcs, out, ocs, k, acc,
-                                        prim, src, b, bg, o, stage, dt,
-                                        cfl ? 1 : 0, i0, i1, i2, st);
+        k_stage<1, T><<<grid, 256, 0, s>>>(un, ucs, us, tcs, out, ocs, k, acc,
+                                           prim, src, b, bg, o, stage, dt, pf,
+                                           cf, i0, i1, i2, st);
     else
-        k_stage<2><<<grid, 256, 0, s>>>(un, ucs, us, tcs, out, ocs, k, acc,
-                                        prim, src, b, bg, o, stage, dt,
-                                        cfl ? 1 : 0, i0, i1, i2, st);
+        k_stage<2, T><<<grid, 256, 0, s>>>(un, ucs, us, tcs, out, ocs, k, acc,
+                                           prim, src, b, bg, o, stage, dt, pf,
+                                           cf, i0, i1, i2, st);
 }
 
 void launch_max_inv_dt(const double *state, const BoxDev &b,
@@ -1122,6 +1310,12 @@ void launch_residual_probe(const double *state, const BoxDev &b,
                            int j, int k, double *out, cudaStream_t s)
 {
     k_residual_probe<<<1, 1, 0, s>>>(state, b, bg, o, i, j, k, out);
+}
+
+void launch_widen(const float *in, int64_t n, double *out, int64_t ocs,
+                  cudaStream_t s)
+{
+    k_widen<<<grid_for(5 * n, 256), 256, 0, s>>>(in, n, out, ocs);
 }
 
 void launch_eval_background(int64_t n, const double *xyz,
@@ -1142,5 +1336,26 @@ void launch_eval_con2prim(int64_t n, const double *cons, const double *gUU,
                                                            prim, ok, iters,
                                                            resid);
 }
+
+#define GRHD_INSTANTIATE(T)                                                   \
+    template void launch_fill_ghosts<T>(double *, T *, const BoxDev &,        \
+                                        const Background &, const Options &,  \
+                                        DevStatus *, cudaStream_t);           \
+    template void launch_cells<T>(const double *, T *, T *, const BoxDev &,   \
+                                  const Background &, const Options &,        \
+                                  DevStatus *, cudaStream_t);                 \
+    template void launch_faces<T>(const T *, const T *, T *, const BoxDev &,  \
+                                  const Background &, const Options &,        \
+                                  const double *, int, double *,              \
+                                  cudaStream_t);                              \
+    template void launch_stage<T>(int, const double *, int64_t,               \
+                                  const double *, int64_t, double *, int64_t, \
+                                  const T *, double *, T *, T *, bool,        \
+                                  const BoxDev &, const Background &,         \
+                                  const Options &, int, double, bool,         \
+                                  const double *, DevStatus *, cudaStream_t);
+
+GRHD_INSTANTIATE(double)
+GRHD_INSTANTIATE(float)
 
 } // namespace grhd

@@ -7,16 +7,17 @@
 namespace grhd {
 
 // One box of the level on the device: interior [lo,hi], ghosted storage
-// [glo,ghi], non-periodic domain [dlo,dhi]; cs / rcs are the component
-// strides of the state (11 components over the ghosted box) and of
-// interior-box arrays (5 components).
+// [glo,ghi], non-periodic domain [dlo,dhi]; cs / rcs / pcs are the
+// component strides of the state (11 components over the ghosted box), of
+// interior-box arrays (5 components) and of the primitive cache (5
+// components over the ghosted box).
 struct BoxDev
 {
     int lo[3], hi[3], glo[3], ghi[3], dlo[3], dhi[3];
     int gn[3], in[3];
     int64_t cs;  // state component stride
     int64_t rcs; // interior array component stride
-    int64_t pcs; // primitive scratch component stride (ghosted volume)
+    int64_t pcs; // primitive cache component stride (ghosted volume)
 
     __host__ __device__ int64_t gidx(int i, int j, int k) const
     {
@@ -71,25 +72,36 @@ constexpr int kPW = kTC + 4; // primitive tile width (2 halo each side)
 constexpr int kGW = kTC + 2; // geometry tile width (1 halo each side)
 constexpr int kGeoFields = 16;
 
-size_t face_kernel_smem_bytes();
-// Per-device kernel attributes (dynamic shared memory of the face kernel).
+// Per-device kernel attributes (dynamic shared memory of the face kernels).
 cudaError_t configure_kernels();
+int64_t face_kernel_blocks(const BoxDev &b, int zchunk);
+
+// T is the arithmetic type of the primitive cache, sources and RHS:
+// double (FP64 path) or float (mixed path).
 
 // Physical ghost fill of the shell, then con2prim of every shell cell into
 // the primitive cache.
-void launch_fill_ghosts(double *state, double *prim, const BoxDev &b,
+template <typename T>
+void launch_fill_ghosts(double *state, T *prim, const BoxDev &b,
                         const Background &bg, const Options &o, DevStatus *st,
                         cudaStream_t s);
 // Interior con2prim into the primitive cache + sources.
-void launch_cells(const double *state, double *prim, double *src,
-                  const BoxDev &b, const Background &bg, const Options &o,
-                  DevStatus *st, cudaStream_t s);
-void launch_faces(const double *prim, const double *src, double *rhs,
-                  const BoxDev &b, const Background &bg, const Options &o,
-                  const double inv_dx[3], int zchunk, cudaStream_t s);
-// Strides: dcs / scs / ucs / ocs / tcs are the component strides of the
-// state-layout arrays each launcher names (11 components over the ghosted
-// box, indexed by BoxDev::gidx); b.rcs is the stride of rhs / k / acc.
+template <typename T>
+void launch_cells(const double *state, T *prim, T *src, const BoxDev &b,
+                  const Background &bg, const Options &o, DevStatus *st,
+                  cudaStream_t s);
+// Face fluxes + divergence + sources -> rhs.  mdot_part (one double per
+// block) receives the block sums of the accretion-rate faces when
+// o.accretion_radius > 0.
+template <typename T>
+void launch_faces(const T *prim, const T *src, T *rhs, const BoxDev &b,
+                  const Background &bg, const Options &o,
+                  const double inv_dx[3], int zchunk, double *mdot_part,
+                  cudaStream_t s);
+// acc[0] = sum of part[0..n); acc[1] += weight * acc[0]
+void launch_mdot_sum(const double *part, int64_t n, double weight,
+                     double *acc, cudaStream_t s);
+// update_conserved (FP64): dst = src + dt rhs, then recovery when asked.
 void launch_update(double *dst, int64_t dcs, const double *src_state,
                    int64_t scs, const double *rhs, const BoxDev &b,
                    const Background &bg, const Options &o, double dt,
@@ -97,12 +109,14 @@ void launch_update(double *dst, int64_t dcs, const double *src_state,
 void launch_recover(double *state, const BoxDev &b, const Background &bg,
                     const Options &o, DevStatus *st, cudaStream_t s);
 // Integrator stage fused with the post-update recovery; mode 0 RK4 stage
-// `stage`, 1 Euler update, 2 SSPRK2 combine.  With prim/src non-null the
-// stage also prepares the next RHS (primitive cache and sources); with cfl
-// it accumulates the next max inverse dt into st->maxinv_bits.
+// `stage`, 1 Euler update, 2 SSPRK2 combine.  With prep the stage also
+// prepares the next RHS (primitive cache and sources); the mixed path
+// reads its con2prim start from `prim` either way.  With cfl it
+// accumulates the next max inverse dt into st->maxinv_bits.
+template <typename T>
 void launch_stage(int mode, const double *un, int64_t ucs, const double *us,
-                  int64_t tcs, double *out, int64_t ocs, const double *k,
-                  double *acc, double *prim, double *src, const BoxDev &b,
+                  int64_t tcs, double *out, int64_t ocs, const T *k,
+                  double *acc, T *prim, T *src, bool prep, const BoxDev &b,
                   const Background &bg, const Options &o, int stage,
                   double dt, bool cfl, const double inv_dx[3], DevStatus *st,
                   cudaStream_t s);
@@ -112,6 +126,9 @@ void launch_max_inv_dt(const double *state, const BoxDev &b,
 void launch_residual_probe(const double *state, const BoxDev &b,
                            const Background &bg, const Options &o, int i,
                            int j, int k, double *out, cudaStream_t s);
+// FP32 5-component interior array into an FP64 one with stride ocs.
+void launch_widen(const float *in, int64_t n, double *out, int64_t ocs,
+                  cudaStream_t s);
 void launch_eval_background(int64_t n, const double *xyz,
                             const Background &bg, double *out,
                             cudaStream_t s);

@@ -172,7 +172,8 @@ class _OperatorBase:
     def __init__(self, eos, background, dx, center, atmosphere,
                  limiter_theta, use_reconstruction, recovery_options,
                  use_static_metric_sources, use_metric_volume_time_sources,
-                 metric_time_derivative_step, excision_radius):
+                 metric_time_derivative_step, excision_radius,
+                 accretion_radius=0.0, precision="fp64"):
         if not dx > 0.0:
             raise ValueError("GRHD grid spacing must be positive")
         self._lib = L.load()
@@ -209,6 +210,12 @@ class _OperatorBase:
         p.use_metric_volume_time_sources = int(use_metric_volume_time_sources)
         p.metric_time_derivative_step = metric_time_derivative_step
         p.excision_radius = excision_radius
+        p.accretion_radius = accretion_radius
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        p.precision = (L.GRHD_PRECISION_MIXED if precision == "mixed"
+                       else L.GRHD_PRECISION_FP64)
+        self.precision = precision
         self.params = p
         self.dx = dx
         self.eos = eos
@@ -335,6 +342,14 @@ class _OperatorBase:
         return {name: (ms[i], n[i])
                 for i, name in enumerate(L.KERNEL_CLASSES)}
 
+    def accretion(self, reset=False):
+        """(Mdot of the last RHS evaluation, its time integral since the
+        last reset) through the sphere r < accretion_radius (new)."""
+        m, i = C.c_double(), C.c_double()
+        self._check(self._lib.grhd_accretion(self._ctx, C.byref(m),
+                                             C.byref(i), int(reset)))
+        return m.value, i.value
+
     def launch_count(self) -> int:
         return int(self._lib.grhd_launch_count(self._ctx))
 
@@ -369,11 +384,12 @@ class FixedBGLevelDataFiniteVolumeOperator(_OperatorBase):
     def __init__(self, eos, background, dx, center,
                  atmosphere=None, limiter_theta=1.5, use_reconstruction=True,
                  recovery_options=None, use_static_metric_sources=True,
-                 excision_radius=0.0):
+                 excision_radius=0.0, accretion_radius=0.0,
+                 precision="fp64"):
         super().__init__(eos, background, dx, center, atmosphere,
                          limiter_theta, use_reconstruction, recovery_options,
                          use_static_metric_sources, False, 1.0e-3,
-                         excision_radius)
+                         excision_radius, accretion_radius, precision)
 
     def compute_rhs(self, rhs, state, domain=None, inverse_dx_U=None):
         self._compute_rhs(rhs, state, inverse_dx_U, 0.0)
@@ -407,12 +423,14 @@ class TimeDependentFixedBGLevelDataFiniteVolumeOperator(_OperatorBase):
                  atmosphere=None, limiter_theta=1.5, use_reconstruction=True,
                  recovery_options=None, use_static_metric_sources=True,
                  use_metric_volume_time_sources=True,
-                 metric_time_derivative_step=1.0e-3, excision_radius=0.0):
+                 metric_time_derivative_step=1.0e-3, excision_radius=0.0,
+                 accretion_radius=0.0, precision="fp64"):
         super().__init__(eos, background_factory, dx, center, atmosphere,
                          limiter_theta, use_reconstruction, recovery_options,
                          use_static_metric_sources,
                          use_metric_volume_time_sources,
-                         metric_time_derivative_step, excision_radius)
+                         metric_time_derivative_step, excision_radius,
+                         accretion_radius, precision)
 
     def compute_rhs(self, rhs, state, domain=None, inverse_dx_U=None,
                     time=0.0):

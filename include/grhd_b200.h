@@ -74,6 +74,18 @@ typedef enum grhd_error_where
     GRHD_WHERE_CFL = 4                /* CFL speed,      :383-390 */
 } grhd_error_where;
 
+/* Arithmetic of the operator (new; the reference is FP64 throughout).
+ * FP64: every quantity in FP64, the reference's algorithm (parity path).
+ * MIXED: reconstruction, HLLE, metric and sources in FP32; con2prim (FP64
+ * Newton started from the previous stage's pressure), the metric within
+ * three gravitational radii of a Kerr-Schild hole, the volume-time source
+ * and the conserved state / RK accumulation in FP64. */
+typedef enum grhd_precision
+{
+    GRHD_PRECISION_FP64 = 0,
+    GRHD_PRECISION_MIXED = 1
+} grhd_precision;
+
 /* Operator parameters: the constructor arguments of the reference operators
  * (:450-464 and :681-700) with the EOS (IdealGasEOS.hpp:13-16), background
  * params_t (KerrSchild.hpp:26-31, CircularBinaryPN.hpp:32-42),
@@ -100,6 +112,10 @@ typedef struct grhd_params
     double metric_time_derivative_step;
     double excision_radius; /* new: cells with coordinate radius below this
                                are frozen and get a zero RHS; <= 0 disables */
+    double accretion_radius; /* new: > 0 turns on the rest-mass accretion
+                                rate through the sphere r < R (see
+                                grhd_accretion) */
+    int precision;           /* new: grhd_precision */
 } grhd_params;
 
 /* One box of the level.  lo/hi: the box's valid cells (inclusive); ghost:
@@ -283,6 +299,20 @@ int grhd_perturb_density(grhd_ctx *ctx, double *state,
                          int64_t state_comp_stride, const grhd_box *box,
                          double amplitude, uint64_t seed, double time,
                          void *stream);
+
+/* ---- accretion rate (new) ---- */
+
+/* With params.accretion_radius = R > 0 every RHS evaluation also computes
+ * the rest-mass accretion rate through the voxelised sphere r < R,
+ *   Mdot = - sum over the faces between a cell inside and a cell outside
+ *          sqrt(det gamma_face) F_D . n_out dx^2,
+ * from the scheme's own HLLE face fluxes (so Mdot is the discrete rest-mass
+ * budget of the sphere), and the integrators accumulate its time integral
+ * with their stage weights (RK4: dt/6 (1,2,2,1); SSPRK2: dt/2, dt/2).
+ * Reads Mdot of the last RHS evaluation and the integral (either may be
+ * NULL) and, with reset != 0, zeroes the integral.  Synchronous. */
+int grhd_accretion(grhd_ctx *ctx, double *mdot_last, double *integral,
+                   int reset);
 
 /* ---- instrumentation ---- */
 

@@ -996,10 +996,17 @@ static int fill_outflow(const orc_params *o, const orc_box *b,
  * 255-298, 322-363), with the time-dependent volume source of :616-675.
  * lo/hi: the box's interior; glo/ghi: its ghosted box; rhs is indexed over
  * the interior box of the whole array `b` via rhs_index. */
+static int inside_sphere(const orc_params *o, int i, int j, int k)
+{
+    double x, y, z;
+    cell_position(o, i, j, k, &x, &y, &z);
+    return sqrt(x * x + y * y + z * z) < o->accretion_radius;
+}
+
 static int box_rhs(const orc_params *o, const orc_box *b, const int lo[3],
                    const int hi[3], double *state, double *rhs,
                    int64_t rcs, const orc_box *rb, const double inv_dx[3],
-                   double t, int do_outflow, orc_error *err)
+                   double t, int do_outflow, orc_error *err, double *mdot)
 {
     int glo[3], ghi[3];
     for (int d = 0; d < 3; ++d)
@@ -1107,6 +1114,23 @@ static int box_rhs(const orc_params *o, const orc_box *b, const int lo[3],
                             &prims[GIDX(ri, rj, rk)],
                             &slopes[GIDX(li, lj, lk)],
                             &slopes[GIDX(ri, rj, rk)], &gf, dir);
+                        /* new: rest-mass flux through the faces of the
+                         * voxelised sphere r < R, each face once (as the
+                         * high face of its left cell) */
+                        if (mdot && side == 0 && o->accretion_radius > 0.0)
+                        {
+                            const int in_l = inside_sphere(o, li, lj, lk);
+                            const int in_r = inside_sphere(o, ri, rj, rk);
+                            if (in_l != in_r)
+                            {
+                                const double sg = sqrt(det_sym(gf.gLL));
+                                const double dA = o->dx * o->dx;
+                                /* outward normal +d when the left cell is
+                                 * inside; Mdot = - outward flux */
+                                *mdot += (in_l ? -1.0 : 1.0) * sg *
+                                         fx[side].D * dA;
+                            }
+                        }
                     }
                     const int64_t g = GIDX(i, j, k);
                     const double idx_d = inv_dx[dir];
@@ -1229,7 +1253,7 @@ int orc_compute_rhs(const orc_params *p, const orc_box *box, double *state,
     if (!check_box(box) || !(p->dx > 0.0))
         return ORC_ERR_INVALID_ARG;
     return box_rhs(p, box, box->lo, box->hi, state, rhs, rcs, box, inv_dx,
-                   time, 1, err);
+                   time, 1, err, NULL);
 }
 
 typedef struct
@@ -1252,8 +1276,22 @@ static void *slab_worker(void *arg)
     SlabJob *j = (SlabJob *)arg;
     memset(&j->err, 0, sizeof(j->err));
     j->status = box_rhs(j->p, j->box, j->lo, j->hi, j->state, j->rhs, j->rcs,
-                        j->box, j->inv_dx, j->time, 0, &j->err);
+                        j->box, j->inv_dx, j->time, 0, &j->err, NULL);
     return NULL;
+}
+
+int orc_compute_rhs_mdot(const orc_params *p, const orc_box *box,
+                         double *state, double *rhs, int64_t rcs,
+                         const double inv_dx[3], double time, double *mdot,
+                         orc_error *err)
+{
+    if (err)
+        memset(err, 0, sizeof(*err));
+    if (!check_box(box) || !(p->dx > 0.0))
+        return ORC_ERR_INVALID_ARG;
+    *mdot = 0.0;
+    return box_rhs(p, box, box->lo, box->hi, state, rhs, rcs, box, inv_dx,
+                   time, 1, err, mdot);
 }
 
 int orc_compute_rhs_slabs(const orc_params *p, const orc_box *box,
@@ -1567,6 +1605,17 @@ int orc_advance_ssprk2(const orc_params *o, const orc_box *b, double *state,
                        const double inv_dx[3], double t, double dt,
                        orc_diag *diag, orc_error *err)
 {
+    return orc_advance_ssprk2_mdot(o, b, state, inv_dx, t, dt, diag, err,
+                                   NULL);
+}
+
+/* SSPRK2 with the time integral of the accretion rate: U^{n+1} = U^n +
+ * dt/2 L(U^n) + dt/2 L(U^1), so each stage's Mdot carries weight dt/2. */
+int orc_advance_ssprk2_mdot(const orc_params *o, const orc_box *b,
+                            double *state, const double inv_dx[3], double t,
+                            double dt, orc_diag *diag, orc_error *err,
+                            double *mdot_integral)
+{
     const size_t ns = box_state_doubles(b);
     const size_t nr = box_interior_cells(b);
     double *old_state = (double *)malloc(ns * sizeof(double));
@@ -1575,12 +1624,16 @@ int orc_advance_ssprk2(const orc_params *o, const orc_box *b, double *state,
     double *r1 = (double *)malloc(5 * nr * sizeof(double));
     memcpy(old_state, state, ns * sizeof(double));
     memcpy(stage, state, ns * sizeof(double));
-    int st = orc_compute_rhs(o, b, state, r0, nr, inv_dx, t, err);
+    double m0 = 0.0, m1 = 0.0;
+    int st = orc_compute_rhs_mdot(o, b, state, r0, nr, inv_dx, t, &m0, err);
     if (st == ORC_OK)
     {
         orc_update_conserved(o, b, stage, r0, nr, dt, t + dt, 1, diag);
-        st = orc_compute_rhs(o, b, stage, r1, nr, inv_dx, t + dt, err);
+        st = orc_compute_rhs_mdot(o, b, stage, r1, nr, inv_dx, t + dt, &m1,
+                                  err);
     }
+    if (mdot_integral)
+        *mdot_integral += 0.5 * dt * m0 + 0.5 * dt * m1;
     if (st == ORC_OK)
     {
         /* combine_ssprk2_conserved_state, FArrayBoxFiniteVolume.hpp:942-969 */
@@ -1619,6 +1672,16 @@ int orc_advance_rk4(const orc_params *o, const orc_box *b, double *state,
                     const double inv_dx[3], double t, double dt,
                     orc_diag *diag, orc_error *err)
 {
+    return orc_advance_rk4_mdot(o, b, state, inv_dx, t, dt, diag, err, NULL);
+}
+
+/* RK4 with the time integral of the accretion rate, weights dt/6 (1, 2, 2,
+ * 1) -- the weights the stage fluxes carry in U^{n+1}. */
+int orc_advance_rk4_mdot(const orc_params *o, const orc_box *b, double *state,
+                         const double inv_dx[3], double t, double dt,
+                         orc_diag *diag, orc_error *err,
+                         double *mdot_integral)
+{
     const size_t ns = box_state_doubles(b);
     const size_t nr = box_interior_cells(b);
     double *stage = (double *)malloc(ns * sizeof(double));
@@ -1631,10 +1694,13 @@ int orc_advance_rk4(const orc_params *o, const orc_box *b, double *state,
     memcpy(stage, state, ns * sizeof(double));
     for (int s = 0; s < 4 && st == ORC_OK; ++s)
     {
-        st = orc_compute_rhs(o, b, s == 0 ? state : stage, k, nr, inv_dx,
-                             t_stage[s], err);
+        double ms = 0.0;
+        st = orc_compute_rhs_mdot(o, b, s == 0 ? state : stage, k, nr, inv_dx,
+                                  t_stage[s], &ms, err);
         if (st != ORC_OK)
             break;
+        if (mdot_integral)
+            *mdot_integral += (dt / 6.0) * ((s == 1 || s == 2) ? 2.0 : 1.0) * ms;
         for (int kk = b->lo[2]; kk <= b->hi[2]; ++kk)
             for (int j = b->lo[1]; j <= b->hi[1]; ++j)
                 for (int i = b->lo[0]; i <= b->hi[0]; ++i)
@@ -1712,6 +1778,7 @@ void orc_default_params(orc_params *p)
     p->use_metric_volume_time_sources = 0;
     p->metric_time_derivative_step = 1.0e-3;
     p->excision_radius = 0.0;
+    p->accretion_radius = 0.0;
 }
 
 void orc_background_vars(const orc_params *p, double t, double x, double y,

@@ -90,6 +90,7 @@ typedef struct orc_params
         use_metric_volume_time_sources;
     double metric_time_derivative_step;
     double excision_radius;    /* new: <= 0 disables excision */
+    double accretion_radius;   /* new: sphere of the Mdot diagnostic */
 } orc_params;
 
 /* A box of the level: interior cell range (inclusive, Chombo Box), the
@@ -159,6 +160,22 @@ int orc_update_conserved(const orc_params *p, const orc_box *box,
 int orc_advance_ssprk2(const orc_params *p, const orc_box *box, double *state,
                        const double inv_dx[3], double time, double dt,
                        orc_diag *diag, orc_error *err);
+/* New: the RHS plus the rest-mass accretion rate through the voxelised
+ * sphere r < accretion_radius: Mdot = - sum over its boundary faces of
+ * sqrt(det gamma_face) F_D . n_out dx^2, with the scheme's HLLE face
+ * fluxes. */
+int orc_compute_rhs_mdot(const orc_params *p, const orc_box *box,
+                         double *state, double *rhs, int64_t rhs_comp_stride,
+                         const double inv_dx[3], double time, double *mdot,
+                         orc_error *err);
+int orc_advance_ssprk2_mdot(const orc_params *p, const orc_box *box,
+                            double *state, const double inv_dx[3],
+                            double time, double dt, orc_diag *diag,
+                            orc_error *err, double *mdot_integral);
+int orc_advance_rk4_mdot(const orc_params *p, const orc_box *box,
+                         double *state, const double inv_dx[3], double time,
+                         double dt, orc_diag *diag, orc_error *err,
+                         double *mdot_integral);
 /* New: classic RK4 with post-stage recovery. */
 int orc_advance_rk4(const orc_params *p, const orc_box *box, double *state,
                     const double inv_dx[3], double time, double dt,

@@ -157,7 +157,7 @@ CASES = {
 }
 
 
-def gpu_operator(p):
+def gpu_operator(p, precision="fp64"):
     """The product operator with the oracle case's settings."""
     import grdzhadzha_b200 as G
     eos = G.IdealGasEOS(p.gamma)
@@ -173,7 +173,8 @@ def gpu_operator(p):
             eos, bg, p.dx, center, atmo, p.limiter_theta,
             bool(p.use_reconstruction), rec,
             bool(p.use_static_metric_sources), False,
-            p.metric_time_derivative_step, p.excision_radius)
+            p.metric_time_derivative_step, p.excision_radius,
+            p.accretion_radius, precision)
     bg = G.CircularBinaryPN(mass_1=p.pn_mass_1, mass_2=p.pn_mass_2,
                             separation=p.pn_separation,
                             angular_velocity=p.pn_angular_velocity,
@@ -183,7 +184,8 @@ def gpu_operator(p):
         eos, bg, p.dx, center, atmo, p.limiter_theta,
         bool(p.use_reconstruction), rec, bool(p.use_static_metric_sources),
         bool(p.use_metric_volume_time_sources),
-        p.metric_time_derivative_step, p.excision_radius)
+        p.metric_time_derivative_step, p.excision_radius, p.accretion_radius,
+        precision)
 
 
 def gpu_level(box, state_np, device="cuda"):

@@ -45,6 +45,7 @@ class Params(C.Structure):
         ("use_metric_volume_time_sources", C.c_int),
         ("metric_time_derivative_step", C.c_double),
         ("excision_radius", C.c_double),
+        ("accretion_radius", C.c_double),
     ]
 
 
@@ -120,6 +121,14 @@ def lib():
                                           C.c_double, dp, C.c_int, dp]
         L.orc_compute_rhs.argtypes = [P, B, dp, dp, i64, dp, C.c_double,
                                       C.POINTER(Error)]
+        L.orc_compute_rhs_mdot.argtypes = [P, B, dp, dp, i64, dp,
+                                           C.c_double, dp, C.POINTER(Error)]
+        L.orc_advance_ssprk2_mdot.argtypes = [P, B, dp, dp, C.c_double,
+                                              C.c_double, C.POINTER(Diag),
+                                              C.POINTER(Error), dp]
+        L.orc_advance_rk4_mdot.argtypes = [P, B, dp, dp, C.c_double,
+                                           C.c_double, C.POINTER(Diag),
+                                           C.POINTER(Error), dp]
         L.orc_compute_rhs_slabs.argtypes = [P, B, dp, dp, i64, dp,
                                             C.c_double, C.c_int,
                                             C.POINTER(Error)]
@@ -230,6 +239,34 @@ def compute_rhs(p, box, state, time=0.0, inv_dx=None):
     if st:
         raise OracleError(st, err)
     return rhs
+
+
+def compute_rhs_mdot(p, box, state, time=0.0):
+    """(rhs, Mdot through the voxelised sphere r < p.accretion_radius)."""
+    n = interior_cells(box)
+    rhs = np.zeros(5 * n, dtype=np.float64)
+    inv = np.array([1.0 / p.dx] * 3)
+    m = C.c_double()
+    err = Error()
+    st = lib().orc_compute_rhs_mdot(C.byref(p), C.byref(box), _dp(state),
+                                    _dp(rhs), n, _dp(inv), time, C.byref(m),
+                                    C.byref(err))
+    if st:
+        raise OracleError(st, err)
+    return rhs, m.value
+
+
+def advance_mdot(p, box, state, time, dt, method="rk4"):
+    """One step; returns (diag, time integral of Mdot over the step)."""
+    d, err, m = Diag(), Error(), C.c_double(0.0)
+    inv = np.array([1.0 / p.dx] * 3)
+    fn = (lib().orc_advance_rk4_mdot if method == "rk4"
+          else lib().orc_advance_ssprk2_mdot)
+    st = fn(C.byref(p), C.byref(box), _dp(state), _dp(inv), time, dt,
+            C.byref(d), C.byref(err), C.byref(m))
+    if st:
+        raise OracleError(st, err)
+    return d, m.value
 
 
 def compute_rhs_slabs(p, box, state, num_slabs, time=0.0):
