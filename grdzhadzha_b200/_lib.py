@@ -114,6 +114,9 @@ SIGNATURES = {
     "grhd_status_string": (C.c_char_p, [C.c_int]),
     "grhd_compute_rhs": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_int64,
                                    _P(Box), _dp, C.c_double, _vp]),
+    "grhd_compute_rhs_static": (C.c_int, [_vp, _vp, C.c_int64, _vp,
+                                          C.c_int64, _P(Box), _dp,
+                                          C.c_double, _vp]),
     "grhd_recover_primitives": (C.c_int, [_vp, _vp, C.c_int64, _P(Box),
                                           C.c_double, _P(Diagnostics), _vp]),
     "grhd_update_conserved": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_int64,

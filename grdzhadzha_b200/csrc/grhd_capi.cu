@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -1099,3 +1100,142 @@ long long grhd_launch_count(const grhd_ctx *ctx)
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// grhd_compute_rhs_static: grhd_compute_rhs with its scratch in a fixed
+// device array instead of context buffers grown by cudaMalloc.
+//
+// Some callers cannot let a library allocate device memory during a run:
+// a host code whose own pool already holds the device memory it budgets
+// (a cudaMalloc there fails or fragments that pool), and a per-box loop
+// that must not stall because cudaFree waits for the whole device.  For
+// them this entry point takes every scratch word from `g_rhs_scratch`, a
+// file-scope device array of fixed size, and allocates nothing.
+//
+// The array is sized for one box of at most kStaticGhostedCells ghosted
+// cells and kStaticInteriorCells interior cells; larger boxes are rejected
+// with GRHD_ERR_INVALID_ARG.  Every call on a device shares the one array,
+// so calls that overlap in time on that device (two streams, two host
+// threads or two contexts) race on it: issue them one after another.
+// Nothing in the array has to start at zero: each word a kernel reads was
+// written earlier in the same call (ghost and interior primitives, sources,
+// the FP32 or strided RHS copy, one accretion partial per face block).
+namespace {
+
+constexpr int64_t kStaticGhostedCells = 65536;  // e.g. 36^3 = 46656
+constexpr int64_t kStaticInteriorCells = 32768; // e.g. 32^3
+constexpr int64_t kStaticMdotBlocks = 4096;
+constexpr int64_t kStaticPrimOff = 0;
+constexpr int64_t kStaticSrcOff = 5 * kStaticGhostedCells;
+constexpr int64_t kStaticKOff = kStaticSrcOff + 5 * kStaticInteriorCells;
+constexpr int64_t kStaticMdotOff = kStaticKOff + 5 * kStaticInteriorCells;
+constexpr int64_t kStaticDoubles = kStaticMdotOff + kStaticMdotBlocks;
+static_assert(kStaticSrcOff % 32 == 0 && kStaticKOff % 32 == 0 &&
+                  kStaticMdotOff % 32 == 0,
+              "static scratch regions start on 256-byte boundaries");
+
+static __device__ __align__(256) double g_rhs_scratch[kStaticDoubles];
+
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mutex;
+double *g_static_addr[kStaticMaxDevices] = {};
+
+// The address of g_rhs_scratch on the current device, looked up once per
+// device.  The first call on a device makes this lookup (which may load the
+// module on that device); later calls only read the cached pointer.
+int static_scratch(grhd_ctx *ctx, double **out)
+{
+    if (ctx->device < 0 || ctx->device >= kStaticMaxDevices)
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, nullptr,
+                         0.0, "device ordinal outside the static scratch "
+                              "table");
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    if (!g_static_addr[ctx->device])
+    {
+        void *p = nullptr;
+        GRHD_CUDA(ctx, cudaGetSymbolAddress(&p, g_rhs_scratch));
+        g_static_addr[ctx->device] = static_cast<double *>(p);
+    }
+    *out = g_static_addr[ctx->device];
+    return GRHD_OK;
+}
+
+template <typename T>
+void enqueue_rhs_static(grhd_ctx *ctx, T *rhs, double *state, const BoxDev &b,
+                        const Background &bg, const double inv_dx[3],
+                        double *base, cudaStream_t s)
+{
+    T *prim = scratch<T>(base + kStaticPrimOff);
+    T *src = scratch<T>(base + kStaticSrcOff);
+    double *mdot_part = base + kStaticMdotOff;
+    launch_fill_ghosts<T>(state, prim, b, bg, ctx->opt, ctx->status, s);
+    launch_cells<T>(state, prim, src, b, bg, ctx->opt, ctx->status, s);
+    launch_faces<T>(prim, src, rhs, b, bg, ctx->opt, inv_dx, ctx->zchunk,
+                    mdot_part, s);
+    ctx->launches += 3;
+    if (ctx->params.accretion_radius > 0.0)
+    {
+        ++ctx->launches;
+        launch_mdot_sum(mdot_part, face_kernel_blocks(b, ctx->zchunk), 0.0,
+                        ctx->mdot_acc, s);
+    }
+}
+
+} // namespace
+
+extern "C" int grhd_compute_rhs_static(grhd_ctx *ctx, double *rhs,
+                                       int64_t rhs_cs, double *state,
+                                       int64_t state_cs, const grhd_box *box,
+                                       const double inverse_dx[3], double time,
+                                       void *stream)
+{
+    int st = common_checks(ctx, state, box);
+    if (st)
+        return st;
+    if (!rhs || !inverse_dx)
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "null rhs or inverse_dx");
+    cudaStream_t s = (cudaStream_t)stream;
+    const BoxDev b = make_box(box, state_cs);
+    if ((st = check_strides(ctx, b, state_cs, rhs_cs)))
+        return st;
+    if (b.gvol() > kStaticGhostedCells || b.ivol() > kStaticInteriorCells ||
+        face_kernel_blocks(b, ctx->zchunk) > kStaticMdotBlocks)
+    {
+        char msg[200];
+        std::snprintf(msg, sizeof(msg),
+                      "box too large for the static RHS scratch: %lld "
+                      "ghosted / %lld interior cells (limits %lld / %lld)",
+                      (long long)b.gvol(), (long long)b.ivol(),
+                      (long long)kStaticGhostedCells,
+                      (long long)kStaticInteriorCells);
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, nullptr,
+                         0.0, msg);
+    }
+    double *base = nullptr;
+    if ((st = static_scratch(ctx, &base)) || (st = reset_status(ctx, s)))
+        return st;
+    const Background bg = make_background(ctx->params, time);
+    double *kbuf = base + kStaticKOff;
+    if (ctx->params.precision == GRHD_PRECISION_MIXED)
+    {
+        enqueue_rhs_static<float>(ctx, scratch<float>(kbuf), state, b, bg,
+                                  inverse_dx, base, s);
+        ++ctx->launches;
+        launch_widen(scratch<float>(kbuf), b.ivol(), rhs, rhs_cs, s);
+    }
+    else if (rhs_cs == b.ivol())
+        enqueue_rhs_static<double>(ctx, rhs, state, b, bg, inverse_dx, base,
+                                   s);
+    else
+    {
+        enqueue_rhs_static<double>(ctx, kbuf, state, b, bg, inverse_dx, base,
+                                   s);
+        for (int c = 0; c < 5; ++c)
+            GRHD_CUDA(ctx, cudaMemcpyAsync(rhs + c * rhs_cs,
+                                           kbuf + c * b.ivol(),
+                                           b.ivol() * sizeof(double),
+                                           cudaMemcpyDeviceToDevice, s));
+    }
+    return finish_status(ctx, b, state, bg, s);
+}

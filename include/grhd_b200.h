@@ -166,6 +166,24 @@ int grhd_compute_rhs(grhd_ctx *ctx, double *rhs, int64_t rhs_comp_stride,
                      const grhd_box *box, const double inverse_dx[3],
                      double time, void *stream);
 
+/* grhd_compute_rhs with no device allocation: the same RHS, its scratch
+ * taken from one fixed device array (about 5 MiB) instead of buffers the
+ * context grows with cudaMalloc.  No counterpart in the reference.  For
+ * hosts that cannot let a library allocate device memory mid-run (their
+ * pool holds the memory; cudaFree would wait for the whole device).
+ * Limits: at most 65536 ghosted and 32768 interior cells (e.g. a 32^3 box
+ * with 2 ghosts); larger boxes return GRHD_ERR_INVALID_ARG.  The first
+ * call on each device looks the array up (cudaGetSymbolAddress with that
+ * device current) and caches its address: make one call per device
+ * before any stream capture begins.  All calls on a device share the
+ * array, so calls that overlap in time there (other streams, threads or
+ * contexts) race: issue them one after another. */
+int grhd_compute_rhs_static(grhd_ctx *ctx, double *rhs,
+                            int64_t rhs_comp_stride, double *state,
+                            int64_t state_comp_stride, const grhd_box *box,
+                            const double inverse_dx[3], double time,
+                            void *stream);
+
 /* recover_primitives(state[, time]) -> AtmosphereResetDiagnostics,
  * :506-520 / :728-743.  `diag` may be NULL. */
 int grhd_recover_primitives(grhd_ctx *ctx, double *state,
