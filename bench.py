@@ -51,6 +51,8 @@ def workload_config(n, precision="fp64"):
                   "seed": SEED},
         "atmosphere": {"rho_floor": 1e-10, "pressure_floor": 1e-12,
                        "max_velocity_squared": 0.8},
+        "recovery": {"max_iterations": 80, "pressure_floor": 1e-12,
+                     "max_velocity_squared": 0.9},
         "reconstruction": "MUSCL-MC theta=2", "riemann": "HLLE",
         "integrator": "RK4", "cfl": CFL, "excision_radius": 1.5,
         "l2": "inputs larger than L2 (state 1.5 GB per grid)",
@@ -60,23 +62,13 @@ def workload_config(n, precision="fp64"):
 # ----------------------------------------------------------------- GPU arm
 
 
-def make_operator(G, n, precision="fp64"):
-    dx = 2.0 * HALF_WIDTH / n
-    c = 0.5 * n * dx
-    return G.TimeDependentFixedBGLevelDataFiniteVolumeOperator(
-        G.IdealGasEOS(GAMMA), G.KerrSchild(mass=1.0, spin=SPIN, dx=dx), dx,
-        (c, c, c), G.AtmosphereOptions(1e-10, 1e-12, 0.8), 2.0, True,
-        G.RecoveryOptions(80, 1e-12, 1e-12, 0.8), True, False, 1e-3, 1.5,
-        precision=precision)
-
-
-def build_state(G, op, n, device):
-    lv = G.LevelBox.cube(n, device=device)
-    op.fill_torus(lv, inner_radius=6.0, pressure_max_radius=12.0,
-                  rho_peak=1.0, max_velocity_squared=0.8)
-    op.perturb_density(lv, 1e-3, SEED)
-    op.recover_primitives(lv)
-    return lv
+def build_state(n, precision, device):
+    """The torus workload (grdzhadzha_b200.workloads.kerr_schild_torus):
+    operator and level with the seeded initial data on the device."""
+    from grdzhadzha_b200 import workloads as W
+    return W.kerr_schild_torus(n, spin=SPIN, half_width=HALF_WIDTH,
+                               gamma=GAMMA, seed=SEED, precision=precision,
+                               device=device)
 
 
 class ClockSampler:
@@ -144,13 +136,11 @@ class ClockSampler:
 
 def run_ours(args, rank, world, local_rank):
     import torch
-    import grdzhadzha_b200 as G
 
     device = f"cuda:{local_rank}"
     torch.cuda.set_device(local_rank)
     n = args.n
-    op = make_operator(G, n, args.precision)
-    lv = build_state(G, op, n, device)
+    op, lv = build_state(n, args.precision, device)
     cells = lv.num_cells
     dist = world > 1
     if dist:
@@ -269,6 +259,86 @@ def run_ours(args, rank, world, local_rank):
             "kernel_ms": kernel_ms, "state": lv, "op": op}
 
 
+# ------------------------------------------------------ batched ensemble
+
+
+def run_ensemble(count, steps, warmup, hbm_peak):
+    """The batched ensemble (Michel + Kerr-Schild tori of sizes 32..128^3,
+    one persistent launch per call, replayed from a CUDA graph, launch
+    shape from the autotuner), timed in FP64 and in mixed precision.
+
+    Both runs take the same step sizes, dt = min(CFL dt, 0.7 x the FP64
+    CFL dt of the initial state) per member, so that the mixed run's
+    accretion rates are compared with the FP64 ones at the same times;
+    the CFL speed is still computed in the launch every step."""
+    import torch
+    import grdzhadzha_b200 as G
+    from grdzhadzha_b200 import workloads as W
+
+    out = {}
+    caps = None
+    for prec in ("fp64", "mixed"):
+        members, specs = W.batched_ensemble(count=count, precision=prec)
+        cells = sum(lv.num_cells for _, lv in members)
+        if caps is None:
+            probe = G.Ensemble(members, cfl=CFL)
+            probe.advance(0, use_graph=False)
+            caps = [0.7 * CFL / probe.member_info(i)["max_inverse_dt"]
+                    for i in range(len(members))]
+            del probe
+        ens = G.Ensemble(members, cfl=CFL, max_dt=caps)
+        tune = ens.autotune(trial_steps=1)
+        ens.advance(warmup, use_graph=False)
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        l0 = ens.launch_count()
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            torch.cuda.synchronize()
+            ev0.record()
+            ens.advance(steps, use_graph=True)
+            ev1.record()
+            torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        infos = [ens.member_info(i) for i in range(len(members))]
+        value = cells * steps / (ms / 1e3)
+        out[prec] = {
+            "value": value, "unit": "cell-updates/s", "ms": ms,
+            "steps": steps, "warmup": warmup, "members": len(members),
+            "cells": cells, "tuning": tune, "clocks": clk.summary(),
+            "gpu_launches": ens.launch_count() - l0,
+            "step_frac_of_hbm_roofline":
+                value * BYTES_PER_CELL_UPDATE / 1e9 / hbm_peak,
+            "_info": infos, "_kind": [sp["kind"] for sp in specs],
+            "sizes": sorted({sp["n"] for sp in specs}),
+        }
+        del ens, members
+        torch.cuda.empty_cache()
+
+    def rel(a, b):
+        return abs(a - b) / abs(b) if b != 0.0 else None
+
+    errs = {}
+    a, b = out["mixed"].pop("_info"), out["fp64"].pop("_info")
+    kinds = out["mixed"].pop("_kind")
+    out["fp64"].pop("_kind")
+    for kind in ("michel", "torus"):
+        sel = [i for i, k in enumerate(kinds) if k == kind]
+        for key in ("mdot", "mdot_integral"):
+            e = [rel(a[i][key], b[i][key]) for i in sel]
+            e = [x for x in e if x is not None]
+            errs[f"{kind}_{key}_max_rel_err"] = max(e) if e else None
+        errs[f"{kind}_time_max_rel_err"] = max(
+            rel(a[i]["time"], b[i]["time"]) for i in sel)
+        errs[f"{kind}_max_abs_mdot_fp64"] = max(abs(b[i]["mdot"])
+                                                for i in sel)
+    errs["note"] = ("Michel: Mdot through r = 4 of the transonic inflow; "
+                    "torus: Mdot through r = 2.5, atmosphere inflow only "
+                    "(the tori do not reach r = 2.5 within the run)")
+    out["mixed"]["mdot_error_vs_fp64"] = errs
+    return out
+
+
 # ------------------------------------------------------------ CPU oracle
 
 
@@ -296,7 +366,7 @@ class CpuBaseline:
                              atmo_pressure_floor=1e-12,
                              atmo_max_velocity_squared=0.8,
                              rec_max_iterations=80,
-                             rec_max_velocity_squared=0.8, limiter_theta=2.0,
+                             rec_max_velocity_squared=0.9, limiter_theta=2.0,
                              excision_radius=1.5)
         nz = min(n, 16 * threads)
         box = O.Box()
@@ -355,6 +425,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", choices=["fp64", "mixed"],
                     default="fp64")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip the mixed 256^3 and batched-ensemble legs")
+    ap.add_argument("--ensemble-count", type=int, default=96)
+    ap.add_argument("--ensemble-steps", type=int, default=100)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -399,6 +473,35 @@ def main():
         tdist.init_process_group("nccl", timeout=timedelta(seconds=120),
                                  device_id=torch.device(f"cuda:{local_rank}"))
     res = run_ours(args, rank, world, local_rank)
+    variants = None
+    if rank == 0 and world == 1 and not args.no_variants:
+        import copy
+        import torch
+        hbm_peak = res["roofline"]["peak"]
+        res.pop("state")
+        res.pop("op")
+        torch.cuda.empty_cache()
+        variants = {}
+        if args.precision == "fp64":
+            margs = copy.copy(args)
+            margs.precision = "mixed"
+            mres = run_ours(margs, rank, world, local_rank)
+            variants["mixed"] = {
+                "value": mres["value"], "unit": "cell-updates/s",
+                "ms_per_step": mres["ms"] / args.steps,
+                "speedup_vs_fp64": mres["value"] / res["value"],
+                "e2e": mres["e2e"]["value"], "clocks": mres["clocks"],
+                "gpu_launches": mres["launches"],
+                "step_frac_of_hbm_roofline":
+                    mres["roofline"]["step_frac_of_hbm_roofline"],
+                "kernel_ms": mres["kernel_ms"]}
+            del mres
+            torch.cuda.empty_cache()
+        ens = run_ensemble(args.ensemble_count, args.ensemble_steps,
+                           args.warmup, hbm_peak)
+        ens["mixed"]["speedup_vs_fp64_plain"] = (
+            ens["mixed"]["value"] / res["value"])
+        variants["batched_ensemble"] = ens
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = host_threads()
@@ -423,6 +526,8 @@ def main():
             "cpu_baseline": cpu, "clocks": res["clocks"],
             "gpu_launches": res["launches"], "kernel_ms": res["kernel_ms"],
         }
+        if variants is not None:
+            line["variants"] = variants
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as tdist

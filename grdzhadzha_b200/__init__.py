@@ -11,3 +11,4 @@ from .operator import (  # noqa: F401
     TimeDependentFixedBGLevelDataFiniteVolumeOperator,
 )
 from ._lib import GRHDError, InvalidArgument  # noqa: F401
+from .ensemble import Ensemble  # noqa: F401

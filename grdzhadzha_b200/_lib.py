@@ -95,6 +95,18 @@ NUM_KERNEL_CLASSES = 5
 KERNEL_CLASSES = ("ghosts", "cells", "faces", "stage", "cfl")
 
 
+class EnsembleMember(C.Structure):
+    _fields_ = [("params", Params), ("box", Box), ("state", C.c_void_p),
+                ("state_comp_stride", C.c_int64),
+                ("inverse_dx", C.c_double * 3), ("cfl", C.c_double),
+                ("max_dt", C.c_double), ("time", C.c_double)]
+
+
+class EnsembleTuning(C.Structure):
+    _fields_ = [("zchunk", C.c_int), ("blocks_per_sm", C.c_int),
+                ("ms_per_step", C.c_double)]
+
+
 class Error(C.Structure):
     _fields_ = [("status", C.c_int), ("where", C.c_int),
                 ("cell", C.c_int * 3), ("residual", C.c_double),
@@ -152,6 +164,23 @@ SIGNATURES = {
     "grhd_profile_read": (C.c_int, [_vp, _P(C.c_double), _P(C.c_longlong)]),
     "grhd_launch_count": (C.c_longlong, [_vp]),
     "grhd_accretion": (C.c_int, [_vp, _dp, _dp, C.c_int]),
+    "grhd_ensemble_create": (C.c_int, [_P(EnsembleMember), C.c_int,
+                                       _P(_vp)]),
+    "grhd_ensemble_destroy": (None, [_vp]),
+    "grhd_ensemble_last_error": (C.c_int, [_vp, _P(Error)]),
+    "grhd_ensemble_get_tuning": (C.c_int, [_vp, _P(EnsembleTuning),
+                                           _P(C.c_int)]),
+    "grhd_ensemble_set_tuning": (C.c_int, [_vp, _P(EnsembleTuning)]),
+    "grhd_ensemble_autotune": (C.c_int, [_vp, C.c_int, _P(EnsembleTuning),
+                                         _vp]),
+    "grhd_ensemble_advance": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
+    "grhd_ensemble_member_info": (C.c_int, [_vp, C.c_int, _dp, _dp, _dp,
+                                            _dp, _P(Diagnostics)]),
+    "grhd_ensemble_reset_accretion": (C.c_int, [_vp]),
+    "grhd_ensemble_invalidate": (C.c_int, [_vp]),
+    "grhd_ensemble_set_barrier_test": (C.c_int, [_vp, C.c_uint,
+                                                 C.c_double]),
+    "grhd_ensemble_launch_count": (C.c_longlong, [_vp]),
 }
 
 _lib = None
@@ -193,12 +222,12 @@ def load():
     return lib
 
 
-def check(lib, ctx, status: int):
+def check(lib, ctx, status: int, last_error=None):
     if status == GRHD_OK:
         return
     err = Error()
     if ctx:
-        lib.grhd_last_error(ctx, C.byref(err))
+        (last_error or lib.grhd_last_error)(ctx, C.byref(err))
     if status == GRHD_ERR_INVALID_ARG:
         raise InvalidArgument(status, err)
     raise GRHDError(status, err)

@@ -679,7 +679,8 @@ int grhd_compute_max_inverse_dt(grhd_ctx *ctx, const double *state,
     const Background bg = make_background(ctx->params, time);
     {
         Timed t_(ctx, GRHD_K_CFL, s);
-        launch_max_inv_dt(state, b, bg, ctx->opt, inverse_dx, ctx->status, s);
+        launch_max_inv_dt(state, b, bg, ctx->opt, inverse_dx, ctx->status,
+                          ctx->params.precision == GRHD_PRECISION_MIXED, s);
     }
     st = finish_status(ctx, b, state, bg, s);
     if (st)
@@ -882,7 +883,9 @@ int grhd_advance_rk4_cfl(grhd_ctx *ctx, double *state, int64_t state_cs,
         {
             Timed t_(ctx, GRHD_K_CFL, s);
             launch_max_inv_dt(state, b, bg0, ctx->opt, inverse_dx,
-                              ctx->status, s);
+                              ctx->status,
+                              ctx->params.precision == GRHD_PRECISION_MIXED,
+                              s);
         }
         if ((st = finish_status(ctx, b, state, bg0, s)))
             return st;
@@ -1239,3 +1242,20 @@ extern "C" int grhd_compute_rhs_static(grhd_ctx *ctx, double *rhs,
     }
     return finish_status(ctx, b, state, bg, s);
 }
+
+// Host helpers shared with the ensemble driver (grhd_ensemble.cu).
+namespace grhd {
+namespace host {
+Options options_of(const grhd_params &p) { return make_options(p); }
+Background background_of(const grhd_params &p, double t)
+{
+    return make_background(p, t);
+}
+BoxDev box_of(const grhd_box *b, int64_t state_cs)
+{
+    return make_box(b, state_cs);
+}
+bool box_valid(const grhd_box *b) { return valid_box(b); }
+bool box_whole_domain(const grhd_box *b) { return box_is_domain(b); }
+} // namespace host
+} // namespace grhd

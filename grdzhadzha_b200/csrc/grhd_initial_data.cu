@@ -292,8 +292,8 @@ __device__ __forceinline__ double mi_residual(const MichelConfigDev &c,
 }
 
 // solve_density + bisect_density_root, :230-310 (bounded loops)
-__device__ double mi_density(const MichelConfigDev &c, const MichelConst &k,
-                             double r, bool &ok)
+__device__ double mi_density_sweep(const MichelConfigDev &c,
+                                   const MichelConst &k, double r, bool &ok)
 {
     if (fabs(r - c.sonic_radius) < 1.0e-12)
         return c.sonic_density;
@@ -368,6 +368,36 @@ __device__ double mi_density(const MichelConfigDev &c, const MichelConst &k,
         }
     }
     return 0.5 * (lower + upper);
+}
+
+// Relative half-width of the band around the sonic radius where the
+// sweep above can miss the root (new; no reference counterpart).
+constexpr double kSonicBand = 5.0e-3;
+
+// The sweep's density, or, where the sweep finds no sign change within
+// kSonicBand of the sonic radius (the two density roots meet there, closer
+// than one sample of the sweep), the density of the branch the sweep
+// selects on that side (the root above rho_s inside r_s, below it
+// outside), from the quadratic through the sonic point and that branch's
+// sweep solutions at r_s (1 +- kSonicBand) and r_s (1 +- 2 kSonicBand).
+// New: the reference fails at such radii.
+__device__ double mi_density(const MichelConfigDev &c, const MichelConst &k,
+                             double r, bool &ok)
+{
+    const double rho = mi_density_sweep(c, k, r, ok);
+    const double x = r / c.sonic_radius - 1.0;
+    if (ok || !(fabs(x) < kSonicBand))
+        return rho;
+    const double sg = x < 0.0 ? -1.0 : 1.0;
+    bool o1 = true, o2 = true;
+    const double p1 =
+        mi_density_sweep(c, k, c.sonic_radius * (1.0 + sg * kSonicBand), o1);
+    const double p2 = mi_density_sweep(
+        c, k, c.sonic_radius * (1.0 + 2.0 * sg * kSonicBand), o2);
+    ok = o1 && o2;
+    const double t = fabs(x) / kSonicBand;
+    return 0.5 * (t - 1.0) * (t - 2.0) * c.sonic_density -
+           t * (t - 2.0) * p1 + 0.5 * t * (t - 1.0) * p2;
 }
 
 // make_point + primitive_from_radius + fill_michel_state, :312-372

@@ -38,15 +38,28 @@ __device__ __forceinline__ void record_error(DevStatus *st, int where,
     atomicMin(&st->err_key, key);
 }
 
+// Loads of data that a persistent launch wrote itself in an earlier phase
+// (CG = true) go through L2 (ld.global.cg): the non-coherent read-only path
+// (__ldg) is only valid for data left unchanged for a whole launch.
+template <bool CG, typename T> __device__ __forceinline__ T rd(const T *p)
+{
+    return CG ? __ldcg(p) : *p;
+}
+template <bool CG, typename T> __device__ __forceinline__ T rdro(const T *p)
+{
+    return CG ? __ldcg(p) : __ldg(p);
+}
+
+template <bool CG = false>
 __device__ __forceinline__ Cons load_cons(const double *s, int64_t cs,
                                           int64_t idx)
 {
     Cons c;
-    c.D = s[kD * cs + idx];
-    c.S[0] = s[(kS1 + 0) * cs + idx];
-    c.S[1] = s[(kS1 + 1) * cs + idx];
-    c.S[2] = s[(kS1 + 2) * cs + idx];
-    c.tau = s[kTau * cs + idx];
+    c.D = rd<CG>(&s[kD * cs + idx]);
+    c.S[0] = rd<CG>(&s[(kS1 + 0) * cs + idx]);
+    c.S[1] = rd<CG>(&s[(kS1 + 1) * cs + idx]);
+    c.S[2] = rd<CG>(&s[(kS1 + 2) * cs + idx]);
+    c.tau = rd<CG>(&s[kTau * cs + idx]);
     return c;
 }
 
@@ -71,16 +84,17 @@ __device__ __forceinline__ void store_prim(double *s, int64_t cs, int64_t idx,
     s[(kV1 + 2) * cs + idx] = p.v[2];
 }
 
+template <bool CG = false>
 __device__ __forceinline__ Prim load_prim(const double *s, int64_t cs,
                                           int64_t idx)
 {
     Prim p;
-    p.rho = s[kRho * cs + idx];
-    p.eps = s[kEps * cs + idx];
-    p.p = s[kPress * cs + idx];
-    p.v[0] = s[(kV1 + 0) * cs + idx];
-    p.v[1] = s[(kV1 + 1) * cs + idx];
-    p.v[2] = s[(kV1 + 2) * cs + idx];
+    p.rho = rd<CG>(&s[kRho * cs + idx]);
+    p.eps = rd<CG>(&s[kEps * cs + idx]);
+    p.p = rd<CG>(&s[kPress * cs + idx]);
+    p.v[0] = rd<CG>(&s[(kV1 + 0) * cs + idx]);
+    p.v[1] = rd<CG>(&s[(kV1 + 1) * cs + idx]);
+    p.v[2] = rd<CG>(&s[(kV1 + 2) * cs + idx]);
     return p;
 }
 
@@ -143,6 +157,26 @@ __device__ __forceinline__ void gLL_double(const GeoT<T> &g, double out[6])
         out[q] = double(g.gLL[q]);
 }
 
+// The metric of a cell for its con2prim, floors and p2c, widened to FP64
+// for the solve: the FP64 metric, or the mixed path's, so that every
+// con2prim of a cell within one path sees the same gamma (a state the
+// stage recovery accepted at the velocity cap is accepted again by the
+// next RHS's boundary fill and CFL speed).
+template <typename T>
+__device__ __forceinline__ void cell_metric_d(const Background &bg, double x,
+                                              double y, double z,
+                                              double gLL[6], double gUU[6])
+{
+    GeoT<T> g;
+    metric_T<T, false>(bg, x, y, z, g, nullptr);
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+    {
+        gLL[q] = double(g.gLL[q]);
+        gUU[q] = double(g.gUU[q]);
+    }
+}
+
 // ------------------------------------------------------------ ghost fill
 
 // Enumerates the shell "ghosted box minus interior box" as three slabs:
@@ -198,17 +232,18 @@ __device__ __forceinline__ bool shell_cell(const BoxDev &b, int64_t t, int &i,
 // then, for every shell cell, the ghosted-box con2prim of the RHS into the
 // primitive cache (recover_primitives_from_fixed_background, :33-58).  The
 // fill itself is FP64 in both paths.
-template <typename T>
-__global__ void __launch_bounds__(256)
-    k_fill_ghosts(double *__restrict__ state, T *__restrict__ prim, BoxDev b,
-                  Background bg, Options o, DevStatus *st, int64_t nshell)
+template <typename T, bool CG = false>
+__device__ __forceinline__ void ghost_item(double *__restrict__ state,
+                                           T *__restrict__ prim,
+                                           const BoxDev &b,
+                                           const Background &bg,
+                                           const Options &o, DevStatus *st,
+                                           int64_t t)
 {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-         t < nshell; t += (int64_t)gridDim.x * blockDim.x)
     {
         int i, j, k;
         if (!shell_cell(b, t, i, j, k))
-            continue;
+            return;
         const int iv[3] = {i, j, k};
         int srcc[3] = {i, j, k};
         bool ghost = false;
@@ -229,32 +264,32 @@ __global__ void __launch_bounds__(256)
         double x, y, z;
         const int64_t idx = b.gidx(i, j, k);
         cell_xyz(o, i, j, k, x, y, z);
-        Geo tg;
-        background_metric<false>(bg, x, y, z, tg, nullptr);
+        double tLL[6], tUU[6];
+        cell_metric_d<T>(bg, x, y, z, tLL, tUU);
         Cons c;
         if (ghost)
         {
             double sx, sy, sz;
             cell_xyz(o, srcc[0], srcc[1], srcc[2], sx, sy, sz);
-            Geo sg;
-            background_metric<false>(bg, sx, sy, sz, sg, nullptr);
-            const Cons sc =
-                load_cons(state, b.cs, b.gidx(srcc[0], srcc[1], srcc[2]));
+            double sLL[6], sUU[6];
+            cell_metric_d<T>(bg, sx, sy, sz, sLL, sUU);
+            const Cons sc = load_cons<CG>(state, b.cs,
+                                          b.gidx(srcc[0], srcc[1], srcc[2]));
             Prim pr;
-            if (!con2prim(o, sc, sg.gUU, pr, nullptr, nullptr))
+            if (!con2prim(o, sc, sUU, pr, nullptr, nullptr))
             {
                 record_error(st, 1, idx);
-                continue;
+                return;
             }
-            floors(o, pr, tg.gLL);
+            floors(o, pr, tLL);
             store_prim(state, b.cs, idx, pr);
-            c = p2c(pr, tg.gLL);
+            c = p2c(pr, tLL);
             store_cons(state, b.cs, idx, c);
         }
         else
-            c = load_cons(state, b.cs, idx);
+            c = load_cons<CG>(state, b.cs, idx);
         Prim pr;
-        if (!con2prim(o, c, tg.gUU, pr, nullptr, nullptr))
+        if (!con2prim(o, c, tUU, pr, nullptr, nullptr))
         {
             record_error(st, 2, idx);
             pr.rho = pr.p = 1.0;
@@ -262,6 +297,16 @@ __global__ void __launch_bounds__(256)
         }
         store_pv(prim, b.pcs, idx, pr);
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_fill_ghosts(double *__restrict__ state, T *__restrict__ prim, BoxDev b,
+                  Background bg, Options o, DevStatus *st, int64_t nshell)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+         t < nshell; t += (int64_t)gridDim.x * blockDim.x)
+        ghost_item<T>(state, prim, b, bg, o, st, t);
 }
 
 // Static-metric sources (:255-298) from the floored primitives and, for
@@ -277,10 +322,15 @@ __device__ __forceinline__ ConsT<T> cell_sources(const Options &o,
     ConsT<T> s = zero_cons<T>();
     if (o.use_src)
     {
-        PrimT<T> fp = convert_prim<double, T>(pr);
-        floors(o, fp, f.g.gLL);
-        if (!is_atmo(o, fp, o.src_atmo_factor))
-            s = static_sources(fp, convert_cons<double, T>(c), f);
+        // floors and the atmosphere test in FP64 for both paths, so that
+        // which cells count as atmosphere does not depend on the type
+        double gLL[6];
+        gLL_double(f.g, gLL);
+        Prim fd = pr;
+        floors(o, fd, gLL);
+        if (!is_atmo(o, fd, o.src_atmo_factor))
+            s = static_sources(convert_prim<double, T>(fd),
+                               convert_cons<double, T>(c), f);
     }
     if (o.use_vol && bg.kind == 1)
     {
@@ -307,15 +357,15 @@ __device__ __forceinline__ ConsT<T> cell_sources(const Options &o,
 // k_fill_ghosts) and the sources into the source scratch.  Excised cells
 // keep their frozen primitives and get no source.  The mixed path starts
 // con2prim from the state's stored pressure.
-template <typename T>
-__global__ void __launch_bounds__(256, 2)
-    k_cells(const double *__restrict__ state, T *__restrict__ prim,
-            T *__restrict__ src, BoxDev b, Background bg, Options o,
-            DevStatus *st)
+template <typename T, bool CG = false>
+__device__ __forceinline__ void cells_item(const double *__restrict__ state,
+                                           T *__restrict__ prim,
+                                           T *__restrict__ src,
+                                           const BoxDev &b,
+                                           const Background &bg,
+                                           const Options &o, DevStatus *st,
+                                           int64_t t)
 {
-    const int64_t n = b.ivol();
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
-         t += (int64_t)gridDim.x * blockDim.x)
     {
         const int i = b.lo[0] + (int)(t % b.in[0]);
         const int64_t r = t / b.in[0];
@@ -325,9 +375,9 @@ __global__ void __launch_bounds__(256, 2)
         ConsT<T> s = zero_cons<T>();
         if (excised(o, i, j, k))
         {
-            store_pv(prim, b.pcs, g, load_prim(state, b.cs, g));
+            store_pv(prim, b.pcs, g, load_prim<CG>(state, b.cs, g));
             store_src(src, b.rcs, t, s);
-            continue;
+            return;
         }
         double x, y, z;
         cell_xyz(o, i, j, k, x, y, z);
@@ -336,9 +386,9 @@ __global__ void __launch_bounds__(256, 2)
             metric_T<T, true>(bg, x, y, z, f.g, &f);
         else
             metric_T<T, false>(bg, x, y, z, f.g, nullptr);
-        const Cons c = load_cons(state, b.cs, g);
+        const Cons c = load_cons<CG>(state, b.cs, g);
         Prim pr;
-        if (!cell_con2prim(o, c, f.g, state[kPress * b.cs + g], pr))
+        if (!cell_con2prim(o, c, f.g, rd<CG>(&state[kPress * b.cs + g]), pr))
         {
             record_error(st, 2, g);
             pr.rho = pr.p = 1.0;
@@ -350,6 +400,18 @@ __global__ void __launch_bounds__(256, 2)
         store_pv(prim, b.pcs, g, pr);
         store_src(src, b.rcs, t, s);
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 2)
+    k_cells(const double *__restrict__ state, T *__restrict__ prim,
+            T *__restrict__ src, BoxDev b, Background bg, Options o,
+            DevStatus *st)
+{
+    const int64_t n = b.ivol();
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x)
+        cells_item<T>(state, prim, src, b, bg, o, st, t);
 }
 
 // ----------------------------------------------------------- face pass
@@ -402,14 +464,14 @@ __device__ __forceinline__ void geo_avg_smem(const T *g, int n, int ca, int cb,
         v.shift[i] = T(0.5) * (g[(13 + i) * n + ca] + g[(13 + i) * n + cb]);
 }
 
-template <typename T>
+template <typename T, bool CG = false>
 __device__ __forceinline__ PVT<T> load_pv_global(const T *__restrict__ prim,
                                                  int64_t pcs, int64_t idx)
 {
     PVT<T> p;
 #pragma unroll
     for (int c = 0; c < 5; ++c)
-        p.q[c] = __ldg(&prim[c * pcs + idx]);
+        p.q[c] = rdro<CG>(&prim[c * pcs + idx]);
     return p;
 }
 
@@ -495,14 +557,16 @@ __device__ __forceinline__ void block_partial(double v, double *scratch,
 // buffered by plane; x and y faces from shared memory (each tile also
 // evaluates its two boundary faces per row), the z face from a 4-plane
 // register window (each z face once); divergence + sources to the RHS.
-template <typename T, bool MDOT>
-__global__ void __launch_bounds__(kTB *kTB, 2)
-    k_faces(const T *__restrict__ prim, const T *__restrict__ src,
-            T *__restrict__ rhs, BoxDev b, Background bg, Options o,
-            double idx0_, double idx1_, double idx2_, int zchunk,
-            double *__restrict__ mdot_part)
+// One tile (bx, by, bz) of the face pass; 16x16 threads, `smem_raw` holds
+// faces_smem<T>() bytes; the tile's accretion sum goes to mdot_part[part].
+template <typename T, bool MDOT, bool CG = false>
+__device__ __forceinline__ void
+faces_tile(const T *__restrict__ prim, const T *__restrict__ src,
+           T *__restrict__ rhs, const BoxDev &b, const Background &bg,
+           const Options &o, double idx0_, double idx1_, double idx2_,
+           int zchunk, int bx, int by, int bz, unsigned char *smem_raw,
+           double *__restrict__ mdot_part, int64_t part)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     T *smem = reinterpret_cast<T *>(smem_raw);
     constexpr int nP = kPW * kPW;
     constexpr int nG = kGW * kGW;
@@ -515,9 +579,9 @@ __global__ void __launch_bounds__(kTB *kTB, 2)
 
     const int a = threadIdx.x, bb = threadIdx.y;
     const int tid = bb * kTB + a;
-    const int i0 = b.lo[0] + blockIdx.x * kTC;
-    const int j0 = b.lo[1] + blockIdx.y * kTC;
-    const int k0 = b.lo[2] + blockIdx.z * zchunk;
+    const int i0 = b.lo[0] + bx * kTC;
+    const int j0 = b.lo[1] + by * kTC;
+    const int k0 = b.lo[2] + bz * zchunk;
     const int k1 = min(k0 + zchunk - 1, b.hi[2]);
     const int ci = i0 + a, cj = j0 + bb; // this thread's cell column
     const bool col_ok = a < kTC && bb < kTC && ci <= b.hi[0] && cj <= b.hi[1];
@@ -529,10 +593,10 @@ __global__ void __launch_bounds__(kTB *kTB, 2)
     tile_geometry(Gb, bg, o, i0, j0, k0, tid);
     __syncthreads();
     {
-        w0 = load_pv_global(prim, b.pcs, b.gidx(ci_c, cj_c, k0 - 2));
-        w1 = load_pv_global(prim, b.pcs, b.gidx(ci_c, cj_c, k0 - 1));
-        w2 = load_pv_global(prim, b.pcs, b.gidx(ci_c, cj_c, k0));
-        w3 = load_pv_global(prim, b.pcs, b.gidx(ci_c, cj_c, k0 + 1));
+        w0 = load_pv_global<T, CG>(prim, b.pcs, b.gidx(ci_c, cj_c, k0 - 2));
+        w1 = load_pv_global<T, CG>(prim, b.pcs, b.gidx(ci_c, cj_c, k0 - 1));
+        w2 = load_pv_global<T, CG>(prim, b.pcs, b.gidx(ci_c, cj_c, k0));
+        w3 = load_pv_global<T, CG>(prim, b.pcs, b.gidx(ci_c, cj_c, k0 + 1));
         if (col_ok)
         {
             double x, y, z;
@@ -555,7 +619,7 @@ __global__ void __launch_bounds__(kTB *kTB, 2)
     {
         T *Gc = Gb + cur * kGeoFields * nG;
         T *Gn = Gb + (cur ^ 1) * kGeoFields * nG;
-        w3 = load_pv_global(prim, b.pcs, b.gidx(ci_c, cj_c, k + 2));
+        w3 = load_pv_global<T, CG>(prim, b.pcs, b.gidx(ci_c, cj_c, k + 2));
         // primitive cross tile at plane k (clamped to the ghosted box)
         for (int idx = tid; idx < nP; idx += kTB * kTB)
         {
@@ -567,7 +631,7 @@ __global__ void __launch_bounds__(kTB *kTB, 2)
             const int64_t g = b.gidx(gi, gj, k);
 #pragma unroll
             for (int c = 0; c < 5; ++c)
-                P[c * nP + idx] = __ldg(&prim[c * b.pcs + g]);
+                P[c * nP + idx] = rdro<CG>(&prim[c * b.pcs + g]);
         }
         tile_geometry(Gn, bg, o, i0, j0, k + 1, tid);
         __syncthreads();
@@ -640,7 +704,7 @@ __global__ void __launch_bounds__(kTB *kTB, 2)
                 const T rx = -idx0 * (Fx[c * nFx + fxh] - Fx[c * nFx + fxl]);
                 const T ry = -idx1 * (Fy[c * nFx + fyh] - Fy[c * nFx + fyl]);
                 const T rz = -idx2 * (fh[c] - fl[c]);
-                out[c] = ((rx + ry) + rz) + __ldg(&src[c * b.rcs + ri]);
+                out[c] = ((rx + ry) + rz) + rdro<CG>(&src[c * b.rcs + ri]);
             }
             if (excised(o, ci, cj, k))
             {
@@ -661,10 +725,23 @@ __global__ void __launch_bounds__(kTB *kTB, 2)
     }
     if (MDOT)
         block_partial(macc, reinterpret_cast<double *>(smem_raw), mdot_part,
-                      tid, kTB * kTB,
-                      blockIdx.x + (int64_t)gridDim.x *
-                                       (blockIdx.y + (int64_t)gridDim.y *
-                                                         blockIdx.z));
+                      tid, kTB * kTB, part);
+}
+
+template <typename T, bool MDOT>
+__global__ void __launch_bounds__(kTB *kTB, 2)
+    k_faces(const T *__restrict__ prim, const T *__restrict__ src,
+            T *__restrict__ rhs, BoxDev b, Background bg, Options o,
+            double idx0_, double idx1_, double idx2_, int zchunk,
+            double *__restrict__ mdot_part)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    faces_tile<T, MDOT>(prim, src, rhs, b, bg, o, idx0_, idx1_, idx2_, zchunk,
+                        blockIdx.x, blockIdx.y, blockIdx.z, smem_raw,
+                        mdot_part,
+                        blockIdx.x + (int64_t)gridDim.x *
+                                         (blockIdx.y + (int64_t)gridDim.y *
+                                                           blockIdx.z));
 }
 
 // Mdot of one RHS evaluation: the block partials summed in a fixed order;
@@ -721,6 +798,12 @@ __device__ __forceinline__ void recover_cell(const Options &o, const Geo &g,
     store_cons(out, cs, idx, c);
 }
 
+// Lane of the calling thread in its warp (blocks may be 2-D).
+__device__ __forceinline__ int lane_id()
+{
+    return (int)((threadIdx.x + blockDim.x * threadIdx.y) & 31u);
+}
+
 __device__ __forceinline__ void flush_counts(DevStatus *st,
                                              unsigned long long cnt[4])
 {
@@ -731,7 +814,7 @@ __device__ __forceinline__ void flush_counts(DevStatus *st,
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1)
             v += __shfl_down_sync(0xffffffffu, v, off);
-        if ((threadIdx.x & 31) == 0 && v)
+        if (lane_id() == 0 && v)
             atomicAdd(&st->counts[q], v);
     }
 }
@@ -852,13 +935,44 @@ __device__ __forceinline__ double cell_inverse_dt(const Options &o,
     return cell;
 }
 
-__device__ __forceinline__ void flush_max(DevStatus *st, double v)
+// The CFL speed of a cell from its FP64 con2prim result: floors, the
+// atmosphere test and the characteristic speeds in FP64 for both paths
+// (the mixed path's metric widened), so that the step size does not hinge
+// on whether a near-floor cell rounds to the floor in FP32.
+template <typename T>
+__device__ __forceinline__ double cfl_speed(const Options &o, const Prim &pr,
+                                            const GeoT<T> &g,
+                                            const double inv[3])
+{
+    Geo gd;
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+    {
+        gd.gLL[q] = double(g.gLL[q]);
+        gd.gUU[q] = double(g.gUU[q]);
+    }
+    gd.lapse = double(g.lapse);
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+        gd.shift[q] = double(g.shift[q]);
+    Prim fp = pr;
+    floors(o, fp, gd.gLL);
+    return cell_inverse_dt(o, fp, gd, inv);
+}
+
+__device__ __forceinline__ void flush_max_to(unsigned long long *bits,
+                                             double v)
 {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1)
         v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
-    if ((threadIdx.x & 31) == 0 && v > 0.0)
-        atomicMax(&st->maxinv_bits, (unsigned long long)__double_as_longlong(v));
+    if (lane_id() == 0 && v > 0.0)
+        atomicMax(bits, (unsigned long long)__double_as_longlong(v));
+}
+
+__device__ __forceinline__ void flush_max(DevStatus *st, double v)
+{
+    flush_max_to(&st->maxinv_bits, v);
 }
 
 // One stage of an integrator fused with the post-update recovery
@@ -878,6 +992,136 @@ __device__ __forceinline__ void flush_max(DevStatus *st, double v)
 // 942-969).  The stage input k, the primitive cache and the sources are of
 // type T; U, the accumulator and con2prim are FP64.  The mixed path starts
 // con2prim from the primitive cache's pressure of the same cell.
+template <int MODE, typename T, bool CG = false>
+__device__ __forceinline__ void
+stage_item(const double *un, int64_t ucs, const double *us, int64_t tcs,
+           double *out, int64_t ocs, const T *__restrict__ kv,
+           double *__restrict__ acc, T *__restrict__ prim,
+           T *__restrict__ src, const BoxDev &b, const Background &bg,
+           const Options &o, int stage, double dt, bool prep, bool store_p,
+           bool cfl, const double inv[3], DevStatus *st, int64_t t,
+           unsigned long long cnt[4], double &cell_inv)
+{
+    const double cst = (stage == 2) ? dt : 0.5 * dt;
+    const double dt6 = dt / 6.0;
+    const bool mixed = sizeof(T) != sizeof(double);
+    int i, j, k;
+    interior_cell(b, t, i, j, k);
+    const int64_t g = b.gidx(i, j, k);
+    if (excised(o, i, j, k))
+    {
+        if (out != un)
+            for (int c = 0; c < kStateComps; ++c)
+                out[c * ocs + g] = rd<CG>(&un[c * ucs + g]);
+        if (prep)
+        {
+            store_pv(prim, b.pcs, g, load_prim<CG>(un, ucs, g));
+            store_src(src, b.rcs, t, zero_cons<T>());
+        }
+    }
+    else
+    {
+        const int comp_of[5] = {kD, kS1, kS1 + 1, kS1 + 2, kTau};
+        double u[5];
+#pragma unroll
+        for (int c = 0; c < 5; ++c)
+        {
+            const double kk = double(rd<CG>(&kv[c * b.rcs + t]));
+            const double u0 = rd<CG>(&un[comp_of[c] * ucs + g]);
+            if (MODE == 0)
+            {
+                double a = (stage == 0) ? kk : rd<CG>(&acc[c * b.rcs + t]);
+                if (stage == 1 || stage == 2)
+                    a = a + 2.0 * kk;
+                if (stage < 3)
+                {
+                    acc[c * b.rcs + t] = a;
+                    u[c] = u0 + cst * kk;
+                }
+                else
+                    u[c] = u0 + dt6 * (a + kk);
+            }
+            else if (MODE == 1)
+                u[c] = u0 + dt * kk;
+            else
+                u[c] = 0.5 * (u0 + rd<CG>(&us[comp_of[c] * tcs + g]) + dt * kk);
+        }
+        Cons c;
+        c.D = u[0];
+        c.S[0] = u[1];
+        c.S[1] = u[2];
+        c.S[2] = u[3];
+        c.tau = u[4];
+        double x, y, z;
+        cell_xyz(o, i, j, k, x, y, z);
+        GeoFullT<T> f;
+        if (prep && o.use_src)
+            metric_T<T, true>(bg, x, y, z, f.g, &f);
+        else
+            metric_T<T, false>(bg, x, y, z, f.g, nullptr);
+        double gLL[6];
+        gLL_double(f.g, gLL);
+        const double p_guess =
+            (mixed && prim) ? double(rd<CG>(&prim[1 * b.pcs + g])) : 0.0;
+        // recovery with atmosphere (:60-110)
+        Prim pr;
+        const bool ok = cell_con2prim(o, c, f.g, p_guess, pr);
+        bool reset = !ok;
+        Prim stored;
+        cnt[0] += 1;
+        if (ok)
+        {
+            stored = pr;
+            floors(o, stored, gLL);
+            reset = primitive_differs(pr, stored);
+            if (reset)
+                cnt[2] += 1;
+        }
+        else
+        {
+            cnt[1] += 1;
+            stored = atmosphere(o);
+        }
+        if (reset)
+        {
+            cnt[3] += 1;
+            c = p2c(stored, gLL);
+        }
+        // the RK stage buffer (prep) carries conserved variables
+        // only: its primitive components are never read
+        if (store_p)
+            store_prim(out, ocs, g, stored);
+        store_cons(out, ocs, g, c);
+        if (prep || cfl)
+        {
+            // con2prim of the state just written (unchanged cells:
+            // the same solve on the same input gives pr again)
+            Prim pn = pr;
+            bool okn = ok;
+            if (reset)
+                okn = cell_con2prim(o, c, f.g, stored.p, pn);
+            if (!okn)
+            {
+                record_error(st, cfl && !prep ? 4 : 2,
+                             cfl && !prep ? t : g);
+                pn.rho = pn.p = 1.0;
+                pn.v[0] = pn.v[1] = pn.v[2] = 0.0;
+                pn.eps = 1.0;
+            }
+            if (prep)
+            {
+                store_pv(prim, b.pcs, g, pn);
+                ConsT<T> s = zero_cons<T>();
+                if (okn)
+                    s = cell_sources<T>(o, bg, x, y, z, pn, c, f);
+                store_src(src, b.rcs, t, s);
+            }
+            if (cfl && okn)
+                cell_inv = cfl_speed<T>(o, pn, f.g, inv);
+        }
+    }
+}
+
 template <int MODE, typename T>
 __global__ void __launch_bounds__(256, 2)
     k_stage(const double *un, int64_t ucs, const double *us, int64_t tcs,
@@ -890,137 +1134,16 @@ __global__ void __launch_bounds__(256, 2)
     unsigned long long cnt[4] = {0, 0, 0, 0};
     const int64_t n = b.ivol();
     const int64_t n_pad = (n + blockDim.x - 1) / blockDim.x * blockDim.x;
-    const double cst = (stage == 2) ? dt : 0.5 * dt;
-    const double dt6 = dt / 6.0;
     const double inv[3] = {i0, i1, i2};
     const bool prep = prep_flag != 0 && prim != nullptr;
-    const bool mixed = sizeof(T) != sizeof(double);
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_pad;
          t += (int64_t)gridDim.x * blockDim.x)
     {
         double cell_inv = 0.0;
         if (t < n)
-        {
-            int i, j, k;
-            interior_cell(b, t, i, j, k);
-            const int64_t g = b.gidx(i, j, k);
-            if (excised(o, i, j, k))
-            {
-                if (out != un)
-                    for (int c = 0; c < kStateComps; ++c)
-                        out[c * ocs + g] = un[c * ucs + g];
-                if (prep)
-                {
-                    store_pv(prim, b.pcs, g, load_prim(un, ucs, g));
-                    store_src(src, b.rcs, t, zero_cons<T>());
-                }
-            }
-            else
-            {
-                const int comp_of[5] = {kD, kS1, kS1 + 1, kS1 + 2, kTau};
-                double u[5];
-#pragma unroll
-                for (int c = 0; c < 5; ++c)
-                {
-                    const double kk = double(kv[c * b.rcs + t]);
-                    const double u0 = un[comp_of[c] * ucs + g];
-                    if (MODE == 0)
-                    {
-                        double a = (stage == 0) ? kk : acc[c * b.rcs + t];
-                        if (stage == 1 || stage == 2)
-                            a = a + 2.0 * kk;
-                        if (stage < 3)
-                        {
-                            acc[c * b.rcs + t] = a;
-                            u[c] = u0 + cst * kk;
-                        }
-                        else
-                            u[c] = u0 + dt6 * (a + kk);
-                    }
-                    else if (MODE == 1)
-                        u[c] = u0 + dt * kk;
-                    else
-                        u[c] = 0.5 * (u0 + us[comp_of[c] * tcs + g] + dt * kk);
-                }
-                Cons c;
-                c.D = u[0];
-                c.S[0] = u[1];
-                c.S[1] = u[2];
-                c.S[2] = u[3];
-                c.tau = u[4];
-                double x, y, z;
-                cell_xyz(o, i, j, k, x, y, z);
-                GeoFullT<T> f;
-                if (prep && o.use_src)
-                    metric_T<T, true>(bg, x, y, z, f.g, &f);
-                else
-                    metric_T<T, false>(bg, x, y, z, f.g, nullptr);
-                double gLL[6];
-                gLL_double(f.g, gLL);
-                const double p_guess =
-                    (mixed && prim) ? double(prim[1 * b.pcs + g]) : 0.0;
-                // recovery with atmosphere (:60-110)
-                Prim pr;
-                const bool ok = cell_con2prim(o, c, f.g, p_guess, pr);
-                bool reset = !ok;
-                Prim stored;
-                cnt[0] += 1;
-                if (ok)
-                {
-                    stored = pr;
-                    floors(o, stored, gLL);
-                    reset = primitive_differs(pr, stored);
-                    if (reset)
-                        cnt[2] += 1;
-                }
-                else
-                {
-                    cnt[1] += 1;
-                    stored = atmosphere(o);
-                }
-                if (reset)
-                {
-                    cnt[3] += 1;
-                    c = p2c(stored, gLL);
-                }
-                // the RK stage buffer (prep) carries conserved variables
-                // only: its primitive components are never read
-                if (!prep)
-                    store_prim(out, ocs, g, stored);
-                store_cons(out, ocs, g, c);
-                if (prep || cfl)
-                {
-                    // con2prim of the state just written (unchanged cells:
-                    // the same solve on the same input gives pr again)
-                    Prim pn = pr;
-                    bool okn = ok;
-                    if (reset)
-                        okn = cell_con2prim(o, c, f.g, stored.p, pn);
-                    if (!okn)
-                    {
-                        record_error(st, cfl && !prep ? 4 : 2,
-                                     cfl && !prep ? t : g);
-                        pn.rho = pn.p = 1.0;
-                        pn.v[0] = pn.v[1] = pn.v[2] = 0.0;
-                        pn.eps = 1.0;
-                    }
-                    if (prep)
-                    {
-                        store_pv(prim, b.pcs, g, pn);
-                        ConsT<T> s = zero_cons<T>();
-                        if (okn)
-                            s = cell_sources<T>(o, bg, x, y, z, pn, c, f);
-                        store_src(src, b.rcs, t, s);
-                    }
-                    if (cfl && okn)
-                    {
-                        PrimT<T> fp = convert_prim<double, T>(pn);
-                        floors(o, fp, f.g.gLL);
-                        cell_inv = cell_inverse_dt(o, fp, f.g, inv);
-                    }
-                }
-            }
-        }
+            stage_item<MODE, T>(un, ucs, us, tcs, out, ocs, kv, acc, prim, src,
+                                b, bg, o, stage, dt, prep, !prep, cfl != 0,
+                                inv, st, t, cnt, cell_inv);
         flush_counts(st, cnt);
         cnt[0] = cnt[1] = cnt[2] = cnt[3] = 0;
         if (cfl)
@@ -1031,6 +1154,40 @@ __global__ void __launch_bounds__(256, 2)
 // compute_max_inverse_dt_from_fixed_background (:364-412): per cell
 // con2prim + floors, skip atmosphere, sum_d max|lambda| / dx_d; block max by
 // warp shuffles, one atomicMax per warp on the bit pattern.
+// One cell of the CFL speed in the metric and arithmetic of type T (the
+// FP64 path, or the mixed path as the fused stage computes it).
+template <typename T, bool CG = false>
+__device__ __forceinline__ double cfl_item(const double *__restrict__ state,
+                                           const BoxDev &b,
+                                           const Background &bg,
+                                           const Options &o,
+                                           const double inv[3], DevStatus *st,
+                                           int64_t t)
+{
+    double cell = 0.0;
+    int i, j, k;
+    interior_cell(b, t, i, j, k);
+    if (!excised(o, i, j, k))
+    {
+        double x, y, z;
+        cell_xyz(o, i, j, k, x, y, z);
+        GeoT<T> geo;
+        metric_T<T, false>(bg, x, y, z, geo, nullptr);
+        double gUU[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+            gUU[q] = double(geo.gUU[q]);
+        Prim pr;
+        if (!con2prim(o, load_cons<CG>(state, b.cs, b.gidx(i, j, k)), gUU, pr,
+                      nullptr, nullptr))
+            record_error(st, 4, t);
+        else
+            cell = cfl_speed<T>(o, pr, geo, inv);
+    }
+    return cell;
+}
+
+template <typename T>
 __global__ void __launch_bounds__(256)
     k_max_inv_dt(const double *__restrict__ state, BoxDev b, Background bg,
                  Options o, double i0, double i1, double i2, DevStatus *st)
@@ -1043,26 +1200,7 @@ __global__ void __launch_bounds__(256)
     {
         double cell = 0.0;
         if (t < n)
-        {
-            int i, j, k;
-            interior_cell(b, t, i, j, k);
-            if (!excised(o, i, j, k))
-            {
-                double x, y, z;
-                cell_xyz(o, i, j, k, x, y, z);
-                Geo geo;
-                background_metric<false>(bg, x, y, z, geo, nullptr);
-                Prim pr;
-                if (!con2prim(o, load_cons(state, b.cs, b.gidx(i, j, k)),
-                              geo.gUU, pr, nullptr, nullptr))
-                    record_error(st, 4, t);
-                else
-                {
-                    floors(o, pr, geo.gLL);
-                    cell = cell_inverse_dt(o, pr, geo, inv);
-                }
-            }
-        }
+            cell = cfl_item<T>(state, b, bg, o, inv, st, t);
         flush_max(st, cell);
     }
 }
@@ -1164,6 +1302,325 @@ __global__ void k_eval_con2prim(int64_t n, const double *__restrict__ cons,
         prim[6 * t + 3 + i] = pr.v[i];
 }
 
+// ------------------------------------------------------------- ensemble
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid-wide barrier of the persistent ensemble launch (every block is
+// resident: the launch is cooperative and sized by the occupancy query).
+// Thread 0 of each block arrives on a counter; the last arrival resets it
+// and advances the generation the others wait on.  Each wait is bounded by
+// bar_timeout_ns: a block whose wait runs out sets ctl->error (recording
+// the phase) and every block leaves the kernel.  False on error.
+__device__ bool ens_barrier(const EnsLaunch &a, int phase)
+{
+    EnsControl *c = a.ctl;
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0)
+    {
+        volatile unsigned int *gen = &c->bar_gen;
+        volatile int *err = &c->error;
+        const unsigned int g = *gen;
+        __threadfence();
+        const unsigned int arrived = atomicAdd(&c->bar_count, 1u) + 1u;
+        if (arrived == a.nblocks + a.bar_extra)
+        {
+            atomicExch(&c->bar_count, 0u);
+            __threadfence();
+            atomicAdd(&c->bar_gen, 1u);
+        }
+        else
+        {
+            const unsigned long long t0 = global_ns();
+            while (*gen == g && *err == 0)
+            {
+                if (global_ns() - t0 > a.bar_timeout_ns)
+                {
+                    if (atomicCAS(&c->error, 0, 1) == 0)
+                        c->error_phase = phase;
+                    break;
+                }
+                __nanosleep(128);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *(volatile int *)&a.ctl->error == 0;
+}
+
+// Next work item of phase `phase` for this block.
+__device__ __forceinline__ int64_t ens_next(EnsControl *c, int phase,
+                                            int64_t *sh)
+{
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0)
+        *sh = (int64_t)atomicAdd(&c->ctr[phase % 3], 1ull);
+    __syncthreads();
+    return *sh;
+}
+
+// Member owning item `it` of a prefix-sum table off[0..nm].
+__device__ __forceinline__ int ens_find(const int64_t *off, int nm,
+                                        int64_t it)
+{
+    int lo = 0, hi = nm;
+    while (hi - lo > 1)
+    {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(&off[mid]) <= it)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// dt of a member's step from the CFL speed of the step's input state, as
+// the host driver computes it (cfl / max(speed, 1e-14), capped by max_dt).
+__device__ __forceinline__ double ens_dt(const EnsMember &m,
+                                         unsigned long long step)
+{
+    const double mi =
+        __longlong_as_double((long long)__ldcg(&m.mi_bits[step & 1ull]));
+    double dt = m.cfl / fmax(mi, 1.0e-14);
+    if (m.max_dt > 0.0)
+        dt = fmin(dt, m.max_dt);
+    return dt;
+}
+
+// The persistent ensemble kernel: `steps` RK4 steps of every member.
+// Phase 0: the CFL speed (when need_cfl), interior con2prim + sources and
+// the ghost fill of every state.  Each stage: ghost fill of the stage input
+// (not before the first stage of the launch), face pass into k, stage
+// combination with post-stage recovery, the next RHS's con2prim + sources
+// and (last stage) the next CFL speed; per member one bookkeeping item sums
+// the accretion partials and advances the member time.  The arithmetic of
+// every item is that of the single-box kernels.
+template <typename T>
+__global__ void __launch_bounds__(kEnsItemCells, 2) k_ensemble(EnsLaunch a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(16) EnsMember ms;
+    __shared__ int64_t item_sh;
+    const int tid = threadIdx.y * kTB + threadIdx.x;
+    EnsControl *ctl = a.ctl;
+    const bool lead = blockIdx.x == 0 && tid == 0;
+    const unsigned long long step0 = __ldcg(&ctl->steps_done);
+    const bool need_cfl = __ldcg(&ctl->need_cfl) != 0;
+    const int64_t ncell = __ldg(&a.off_cell[a.nm]);
+    const int64_t nghost = __ldg(&a.off_ghost[a.nm]);
+    const int64_t ntile = __ldg(&a.off_tile[a.nm]);
+    int cur = -1;
+    int ph = 0;
+    auto load = [&](int m) {
+        if (m != cur)
+        {
+            const unsigned long long *src =
+                reinterpret_cast<const unsigned long long *>(a.m + m);
+            unsigned long long *dst =
+                reinterpret_cast<unsigned long long *>(&ms);
+            for (int w = tid; w < (int)(sizeof(EnsMember) / 8);
+                 w += kEnsItemCells)
+                dst[w] = __ldg(&src[w]);
+            __syncthreads();
+            cur = m;
+        }
+    };
+    auto zero_next_mi = [&](unsigned long long step) {
+        for (int m = 0; m < a.nm; ++m)
+            a.m[m].mi_bits[(step + 1ull) & 1ull] = 0ull;
+    };
+
+    // ---- phase 0
+    {
+        const int64_t ncfl = need_cfl ? ncell : 0;
+        if (lead)
+        {
+            ctl->ctr[(ph + 1) % 3] = 0ull;
+            zero_next_mi(step0);
+        }
+        for (;;)
+        {
+            int64_t it = ens_next(ctl, ph, &item_sh);
+            if (it >= ncfl + ncell + nghost)
+                break;
+            if (it < ncfl)
+            {
+                const int m = ens_find(a.off_cell, a.nm, it);
+                load(m);
+                const int64_t t =
+                    (it - __ldg(&a.off_cell[m])) * kEnsItemCells + tid;
+                double v = 0.0;
+                if (t < ms.b.ivol())
+                    v = cfl_item<T, true>(ms.state, ms.b, ms.bg, ms.o, ms.inv,
+                                          ms.st, t);
+                flush_max_to(&ms.mi_bits[step0 & 1ull], v);
+            }
+            else if (it < ncfl + ncell)
+            {
+                it -= ncfl;
+                const int m = ens_find(a.off_cell, a.nm, it);
+                load(m);
+                const int64_t t =
+                    (it - __ldg(&a.off_cell[m])) * kEnsItemCells + tid;
+                if (t < ms.b.ivol())
+                    cells_item<T, true>(ms.state, static_cast<T *>(ms.prim),
+                                        static_cast<T *>(ms.src), ms.b, ms.bg,
+                                        ms.o, ms.st, t);
+            }
+            else
+            {
+                it -= ncfl + ncell;
+                const int m = ens_find(a.off_ghost, a.nm, it);
+                load(m);
+                const int64_t t =
+                    (it - __ldg(&a.off_ghost[m])) * kEnsItemCells + tid;
+                if (t < ms.nshell)
+                    ghost_item<T, true>(ms.state, static_cast<T *>(ms.prim),
+                                        ms.b, ms.bg, ms.o, ms.st, t);
+            }
+        }
+        if (!ens_barrier(a, ph++))
+            return;
+    }
+
+    for (int n = 0; n < a.steps; ++n)
+    {
+        const unsigned long long step = step0 + (unsigned long long)n;
+        for (int s = 0; s < 4; ++s)
+        {
+            // ---- ghost fill of the stage input
+            if (n > 0 || s > 0)
+            {
+                if (lead)
+                {
+                    ctl->ctr[(ph + 1) % 3] = 0ull;
+                    if (s == 0)
+                        zero_next_mi(step);
+                }
+                for (;;)
+                {
+                    const int64_t it = ens_next(ctl, ph, &item_sh);
+                    if (it >= nghost)
+                        break;
+                    const int m = ens_find(a.off_ghost, a.nm, it);
+                    load(m);
+                    const int64_t t =
+                        (it - __ldg(&a.off_ghost[m])) * kEnsItemCells + tid;
+                    if (t < ms.nshell)
+                        ghost_item<T, true>(s == 0 ? ms.state : ms.stage,
+                                            static_cast<T *>(ms.prim),
+                                            s == 0 ? ms.b : ms.sb, ms.bg,
+                                            ms.o, ms.st, t);
+                }
+                if (!ens_barrier(a, ph++))
+                    return;
+            }
+            // ---- face pass
+            if (lead)
+                ctl->ctr[(ph + 1) % 3] = 0ull;
+            for (;;)
+            {
+                const int64_t it = ens_next(ctl, ph, &item_sh);
+                if (it >= ntile)
+                    break;
+                const int m = ens_find(a.off_tile, a.nm, it);
+                load(m);
+                const int64_t local = it - __ldg(&a.off_tile[m]);
+                const int bx = (int)(local % ms.tiles[0]);
+                const int64_t r = local / ms.tiles[0];
+                const int by = (int)(r % ms.tiles[1]);
+                const int bz = (int)(r / ms.tiles[1]);
+                if (ms.has_mdot)
+                    faces_tile<T, true, true>(
+                        static_cast<const T *>(ms.prim),
+                        static_cast<const T *>(ms.src), static_cast<T *>(ms.k),
+                        ms.b, ms.bg, ms.o, ms.inv[0], ms.inv[1], ms.inv[2],
+                        a.zchunk, bx, by, bz, smem_raw, ms.mdot_part, local);
+                else
+                    faces_tile<T, false, true>(
+                        static_cast<const T *>(ms.prim),
+                        static_cast<const T *>(ms.src), static_cast<T *>(ms.k),
+                        ms.b, ms.bg, ms.o, ms.inv[0], ms.inv[1], ms.inv[2],
+                        a.zchunk, bx, by, bz, smem_raw, nullptr, local);
+            }
+            if (!ens_barrier(a, ph++))
+                return;
+            // ---- stage combination (+ bookkeeping items)
+            if (lead)
+                ctl->ctr[(ph + 1) % 3] = 0ull;
+            for (;;)
+            {
+                const int64_t it = ens_next(ctl, ph, &item_sh);
+                if (it >= ncell + a.nm)
+                    break;
+                if (it < ncell)
+                {
+                    const int m = ens_find(a.off_cell, a.nm, it);
+                    load(m);
+                    const int64_t t =
+                        (it - __ldg(&a.off_cell[m])) * kEnsItemCells + tid;
+                    const double dt = ens_dt(ms, step);
+                    unsigned long long cnt[4] = {0ull, 0ull, 0ull, 0ull};
+                    double ci = 0.0;
+                    if (t < ms.b.ivol())
+                        stage_item<0, T, true>(
+                            ms.state, ms.b.cs, nullptr, 0,
+                            s < 3 ? ms.stage : ms.state,
+                            s < 3 ? ms.sb.cs : ms.b.cs,
+                            static_cast<const T *>(ms.k), ms.acc,
+                            static_cast<T *>(ms.prim),
+                            static_cast<T *>(ms.src), ms.b, ms.bg, ms.o, s,
+                            dt, true, s == 3, s == 3, ms.inv, ms.st, t, cnt,
+                            ci);
+                    flush_counts(ms.st, cnt);
+                    if (s == 3)
+                        flush_max_to(&ms.mi_bits[(step + 1ull) & 1ull], ci);
+                }
+                else
+                {
+                    const int m = (int)(it - ncell);
+                    load(m);
+                    const double dt = ens_dt(ms, step);
+                    if (ms.has_mdot)
+                    {
+                        // the single-box k_mdot_sum, 256 threads
+                        const int64_t np = (int64_t)ms.tiles[0] *
+                                           ms.tiles[1] * ms.tiles[2];
+                        double v = 0.0;
+                        for (int64_t q = tid; q < np; q += kEnsItemCells)
+                            v += __ldcg(&ms.mdot_part[q]);
+                        double *w = reinterpret_cast<double *>(smem_raw);
+                        block_partial(v, w, w + 8, tid, kEnsItemCells, 0);
+                        if (tid == 0)
+                        {
+                            const double wgt =
+                                (dt / 6.0) * ((s == 1 || s == 2) ? 2.0 : 1.0);
+                            ms.mdot_acc[0] = w[8];
+                            ms.mdot_acc[1] += wgt * w[8];
+                        }
+                    }
+                    if (s == 3 && tid == 0)
+                        *ms.time += dt;
+                }
+            }
+            if (!ens_barrier(a, ph++))
+                return;
+        }
+    }
+    if (lead)
+    {
+        ctl->steps_done = step0 + (unsigned long long)a.steps;
+        ctl->need_cfl = 0;
+    }
+}
+
 int grid_for(int64_t n, int threads)
 {
     int64_t blocks = (n + threads - 1) / threads;
@@ -1197,8 +1654,47 @@ cudaError_t configure_kernels()
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_faces<float, true>, attr,
                                  (int)faces_smem<float>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_ensemble<double>, attr,
+                                 (int)faces_smem<double>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_ensemble<float>, attr,
+                                 (int)faces_smem<float>());
     return e;
 }
+
+template <typename T> size_t ensemble_smem() { return faces_smem<T>(); }
+
+template <typename T> cudaError_t ensemble_occupancy(int *blocks_per_sm)
+{
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        blocks_per_sm, k_ensemble<T>, kEnsItemCells, faces_smem<T>());
+}
+
+template <typename T>
+cudaError_t launch_ensemble(const EnsLaunch &a, int grid, cudaStream_t s)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kTB, kTB);
+    cfg.dynamicSmemBytes = faces_smem<T>();
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_ensemble<T>, a);
+}
+
+template size_t ensemble_smem<double>();
+template size_t ensemble_smem<float>();
+template cudaError_t ensemble_occupancy<double>(int *);
+template cudaError_t ensemble_occupancy<float>(int *);
+template cudaError_t launch_ensemble<double>(const EnsLaunch &, int,
+                                             cudaStream_t);
+template cudaError_t launch_ensemble<float>(const EnsLaunch &, int,
+                                            cudaStream_t);
 
 int64_t face_kernel_blocks(const BoxDev &b, int zchunk)
 {
@@ -1299,10 +1795,15 @@ void launch_stage(int mode, const double *un, int64_t ucs, const double *us,
 
 void launch_max_inv_dt(const double *state, const BoxDev &b,
                        const Background &bg, const Options &o,
-                       const double inv_dx[3], DevStatus *st, cudaStream_t s)
+                       const double inv_dx[3], DevStatus *st, bool mixed,
+                       cudaStream_t s)
 {
-    k_max_inv_dt<<<grid_for(b.ivol(), 256), 256, 0, s>>>(
-        state, b, bg, o, inv_dx[0], inv_dx[1], inv_dx[2], st);
+    if (mixed)
+        k_max_inv_dt<float><<<grid_for(b.ivol(), 256), 256, 0, s>>>(
+            state, b, bg, o, inv_dx[0], inv_dx[1], inv_dx[2], st);
+    else
+        k_max_inv_dt<double><<<grid_for(b.ivol(), 256), 256, 0, s>>>(
+            state, b, bg, o, inv_dx[0], inv_dx[1], inv_dx[2], st);
 }
 
 void launch_residual_probe(const double *state, const BoxDev &b,

@@ -120,9 +120,12 @@ void launch_stage(int mode, const double *un, int64_t ucs, const double *us,
                   const Background &bg, const Options &o, int stage,
                   double dt, bool cfl, const double inv_dx[3], DevStatus *st,
                   cudaStream_t s);
+// The CFL speed in the FP64 metric and arithmetic, or (mixed) in those of
+// the mixed path's fused stage.
 void launch_max_inv_dt(const double *state, const BoxDev &b,
                        const Background &bg, const Options &o,
-                       const double inv_dx[3], DevStatus *st, cudaStream_t s);
+                       const double inv_dx[3], DevStatus *st, bool mixed,
+                       cudaStream_t s);
 void launch_residual_probe(const double *state, const BoxDev &b,
                            const Background &bg, const Options &o, int i,
                            int j, int k, double *out, cudaStream_t s);
@@ -135,5 +138,69 @@ void launch_eval_background(int64_t n, const double *xyz,
 void launch_eval_con2prim(int64_t n, const double *cons, const double *gUU,
                           const Options &o, double *prim, int *ok, int *iters,
                           double *resid, cudaStream_t s);
+
+// ------------------------------------------------------------ ensemble
+// Many independent boxes (members) advanced by one persistent launch: each
+// phase (ghost fill, face pass, stage) runs the work items of every member,
+// handed out by an atomic counter, between grid-wide barriers.
+
+// Cells per cell-wise work item (one per thread of a 16x16 block).
+constexpr int kEnsItemCells = kTB * kTB;
+
+// One member, as the persistent kernel reads it.  prim/src/k hold the
+// ensemble's arithmetic type T.
+struct EnsMember
+{
+    BoxDev b;  // the member's state box (caller's component stride)
+    BoxDev sb; // the same box over the RK stage buffer (stride = volume)
+    Background bg;
+    Options o;
+    double inv[3];
+    double cfl, max_dt;
+    double *state, *stage, *acc;
+    void *prim, *src, *k;
+    double *mdot_part;           // one partial per face tile
+    double *mdot_acc;            // [Mdot of the last RHS, time integral]
+    double *time;                // member time
+    unsigned long long *mi_bits; // [2] max inverse dt by step parity
+    DevStatus *st;
+    int tiles[3];   // face tiles along x, y, z
+    int has_mdot;
+    int64_t nshell; // ghost shell cells
+};
+
+// Control block of a launch (zeroed by the host before each launch, except
+// steps_done and need_cfl, which carry over between launches).
+struct EnsControl
+{
+    unsigned long long ctr[3]; // work counters, by phase number mod 3
+    unsigned int bar_count, bar_gen;
+    int error;       // 1: a grid barrier wait ran out
+    int error_phase; // phase number of that barrier
+    unsigned long long steps_done;
+    int need_cfl; // the first phase computes the CFL speed
+    int pad_;
+};
+
+struct EnsLaunch
+{
+    const EnsMember *m;
+    int nm;
+    // per-member prefix sums of work items, [nm + 1] each
+    const int64_t *off_ghost, *off_cell, *off_tile;
+    EnsControl *ctl;
+    int steps;
+    int zchunk;
+    unsigned int nblocks;
+    unsigned int bar_extra; // arrivals beyond the grid a barrier waits for
+    unsigned long long bar_timeout_ns;
+};
+
+// Dynamic shared memory and resident blocks per SM of the ensemble kernel.
+template <typename T> size_t ensemble_smem();
+template <typename T> cudaError_t ensemble_occupancy(int *blocks_per_sm);
+// One persistent launch of `grid` blocks (all resident; cooperative).
+template <typename T>
+cudaError_t launch_ensemble(const EnsLaunch &a, int grid, cudaStream_t s);
 
 } // namespace grhd

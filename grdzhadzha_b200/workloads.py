@@ -1,0 +1,119 @@
+"""Seeded synthetic workloads built on the device: Kerr-Schild tori and
+Michel inflows, singly or as the batched ensemble of many of them.
+
+Setups follow the reference's torus and Michel initial data
+(Source/InitialConditions/FixedBGTorus.hpp:291-409,
+Tests/GRHDLevelDataMichelAccretion/GRHDLevelDataMichelAccretion.cpp:
+312-372); sizes, seeds and parameter ranges are this package's choices,
+stated in each function."""
+from __future__ import annotations
+
+import numpy as np
+
+from .operator import (AtmosphereOptions, IdealGasEOS, KerrSchild, LevelBox,
+                       RecoveryOptions,
+                       TimeDependentFixedBGLevelDataFiniteVolumeOperator)
+
+SEED = 20261203
+
+
+def kerr_schild_torus(n, spin=0.9, half_width=40.0, gamma=5.0 / 3.0,
+                      inner_radius=6.0, pressure_max_radius=12.0,
+                      rho_peak=1.0, perturbation=1e-3, seed=SEED + 1,
+                      accretion_radius=0.0, precision="fp64",
+                      device="cuda"):
+    """Constant-angular-momentum torus around a Kerr-Schild hole (M = 1)
+    on an n^3 grid over [-half_width, half_width]^3: atmosphere 1e-10 /
+    1e-12 / v^2 cap 0.8, recovery v^2 cap 0.9, MUSCL-MC (theta 2) + HLLE,
+    excision r < 1.5, density times (1 + perturbation U(-1, 1)).  Returns
+    (operator, level).
+
+    The recovery cap sits above the atmosphere cap: the floors rescale a
+    fast cell's velocity to exactly the atmosphere cap (Atmosphere.hpp:
+    36-40), and with equal caps the next con2prim of that reset state
+    fails whenever rounding puts v^2 on or above the cap."""
+    nn = (n, n, n) if isinstance(n, int) else tuple(n)
+    dx = 2.0 * half_width / nn[0]
+    c = tuple(0.5 * nn[d] * dx for d in range(3))
+    op = TimeDependentFixedBGLevelDataFiniteVolumeOperator(
+        IdealGasEOS(gamma), KerrSchild(mass=1.0, spin=spin, dx=dx), dx, c,
+        AtmosphereOptions(1e-10, 1e-12, 0.8), 2.0, True,
+        RecoveryOptions(80, 1e-12, 1e-12, 0.9), True, False, 1e-3, 1.5,
+        accretion_radius, precision)
+    lv = LevelBox.cube(nn, device=device)
+    op.fill_torus(lv, inner_radius=inner_radius,
+                  pressure_max_radius=pressure_max_radius, rho_peak=rho_peak,
+                  max_velocity_squared=0.8)
+    if perturbation:
+        op.perturb_density(lv, perturbation, seed)
+    op.recover_primitives(lv)
+    return op, lv
+
+
+def michel(n, sonic_radius=8.0, half_width=16.0, gamma=4.0 / 3.0,
+           noise=1e-6, seed=SEED, accretion_radius=0.0, precision="fp64",
+           device="cuda"):
+    """Michel inflow onto a Schwarzschild hole (M = 1) in Kerr-Schild
+    coordinates on an n^3 grid over [-half_width, half_width]^3: sonic
+    density 1e-6, atmosphere inside r = 2.5 and floors 1e-12 / 1e-16,
+    v^2 caps 0.8 (atmosphere) / 0.9 (recovery), MUSCL-MC (theta 2) + HLLE,
+    excision r < 1.5, density times (1 + noise U(-1, 1)).  Returns
+    (operator, level)."""
+    nn = (n, n, n) if isinstance(n, int) else tuple(n)
+    dx = 2.0 * half_width / nn[0]
+    c = tuple(0.5 * nn[d] * dx for d in range(3))
+    op = TimeDependentFixedBGLevelDataFiniteVolumeOperator(
+        IdealGasEOS(gamma), KerrSchild(mass=1.0, spin=0.0, dx=dx), dx, c,
+        AtmosphereOptions(1e-12, 1e-16, 0.8), 2.0, True,
+        RecoveryOptions(100, 1e-12, 1e-16, 0.9), True, False, 1e-3, 1.5,
+        accretion_radius, precision)
+    lv = LevelBox.cube(nn, device=device)
+    op.fill_michel(lv, sonic_radius=sonic_radius, sonic_density=1e-6,
+                   atmosphere_radius=2.5)
+    if noise:
+        op.perturb_density(lv, noise, seed)
+    op.recover_primitives(lv)
+    return op, lv
+
+
+def batched_ensemble(count=96, sizes=(32, 48, 64, 96, 128), seed=SEED + 3,
+                     precision="mixed", device="cuda", max_cells=None):
+    """The batched ensemble: `count` independent members with n drawn
+    uniformly from `sizes`; the first half Michel inflows (sonic radius
+    U[5, 12], half width 2 r_s, Gamma 4/3, accretion sphere r = 4), the
+    second half Kerr-Schild tori (spin U[0, 0.99], inner edge U[6, 10],
+    pressure maximum inner + 6, half width 40, Gamma 4/3 or 5/3, accretion
+    sphere r = 2.5); numpy seeded.  `max_cells` (optional) caps the total
+    cell count by dropping the largest sizes.  Returns (members, specs)."""
+    rng = np.random.default_rng(seed)
+    members, specs = [], []
+    total = 0
+    for i in range(count):
+        n = int(rng.choice(sizes))
+        if max_cells is not None:
+            while n ** 3 + total > max_cells and n > min(sizes):
+                n = max(s for s in sizes if s < n)
+        total += n ** 3
+        if i < count // 2:
+            rs = float(rng.uniform(5.0, 12.0))
+            spec = {"kind": "michel", "n": n, "sonic_radius": rs,
+                    "half_width": 2.0 * rs, "gamma": 4.0 / 3.0,
+                    "seed": int(seed + i)}
+            op, lv = michel(n, sonic_radius=rs, half_width=2.0 * rs,
+                            seed=spec["seed"], accretion_radius=4.0,
+                            precision=precision, device=device)
+        else:
+            a = float(rng.uniform(0.0, 0.99))
+            rin = float(rng.uniform(6.0, 10.0))
+            g = float(rng.choice([4.0 / 3.0, 5.0 / 3.0]))
+            spec = {"kind": "torus", "n": n, "spin": a, "inner_radius": rin,
+                    "pressure_max_radius": rin + 6.0, "gamma": g,
+                    "seed": int(seed + i)}
+            op, lv = kerr_schild_torus(n, spin=a, gamma=g, inner_radius=rin,
+                                       pressure_max_radius=rin + 6.0,
+                                       seed=spec["seed"],
+                                       accretion_radius=2.5,
+                                       precision=precision, device=device)
+        members.append((op, lv))
+        specs.append(spec)
+    return members, specs

@@ -356,6 +356,84 @@ int grhd_profile_read(grhd_ctx *ctx, double ms[GRHD_K_NUM_CLASSES],
 /* Total number of kernels this context has launched. */
 long long grhd_launch_count(const grhd_ctx *ctx);
 
+/* ---- batched ensemble (new; no reference counterpart) ----
+ * Many independent single-box problems on Kerr-Schild backgrounds, of any
+ * sizes, spins, EOS and floors, advanced together: every call runs `steps`
+ * classic RK4 steps of every member (the grhd_advance_rk4_cfl step: dt =
+ * min(cfl / max inverse dt, max_dt) per member, post-stage recovery,
+ * excision, accretion rate) in ONE persistent kernel launch whose phases
+ * (ghost fill, face pass, stage) hand out the work items of all members
+ * between grid-wide barriers.  The launch can be replayed from a CUDA
+ * graph.  Each member's arithmetic is that of the single-box entry points
+ * (FP64 members reproduce grhd_advance_rk4_cfl to rounding, 1e-13 of the
+ * state's scale).  The ensemble runs on its own stream, ordered after and
+ * before `stream`. */
+typedef struct grhd_ensemble grhd_ensemble;
+
+typedef struct grhd_ensemble_member
+{
+    grhd_params params; /* Kerr-Schild; the same precision for all members */
+    grhd_box box;       /* the member's whole domain (box == domain)       */
+    double *state;      /* device, 11 components over the ghosted box      */
+    int64_t state_comp_stride;
+    double inverse_dx[3];
+    double cfl;    /* > 0 */
+    double max_dt; /* <= 0: no cap */
+    double time;   /* initial member time */
+} grhd_ensemble_member;
+
+/* Launch shape of the persistent kernel: the z extent of a face tile and
+ * the resident blocks per SM; ms_per_step is what the autotuner measured
+ * (0 when set by hand). */
+typedef struct grhd_ensemble_tuning
+{
+    int zchunk;
+    int blocks_per_sm;
+    double ms_per_step;
+} grhd_ensemble_tuning;
+
+/* Allocates the scratch of every member (the states stay the caller's).
+ * On error *out is still set (read the message, then destroy it). */
+int grhd_ensemble_create(const grhd_ensemble_member *members, int count,
+                         grhd_ensemble **out);
+void grhd_ensemble_destroy(grhd_ensemble *ens);
+int grhd_ensemble_last_error(const grhd_ensemble *ens, grhd_error *out);
+int grhd_ensemble_get_tuning(const grhd_ensemble *ens,
+                             grhd_ensemble_tuning *tuning,
+                             int *max_blocks_per_sm);
+int grhd_ensemble_set_tuning(grhd_ensemble *ens,
+                             const grhd_ensemble_tuning *tuning);
+/* Times `trial_steps` steps of every candidate launch shape (z chunks 8,
+ * 16, 32, 64 x 1..max blocks per SM) on the real members, keeps the
+ * fastest and restores the states, times, accretion integrals and
+ * counters as they were. */
+int grhd_ensemble_autotune(grhd_ensemble *ens, int trial_steps,
+                           grhd_ensemble_tuning *best, void *stream);
+/* `steps` RK4 steps of every member in one launch; use_graph = 1 replays a
+ * CUDA graph captured for this step count (captured at its first use).
+ * Synchronises; a recovery failure returns GRHD_ERR_RECOVERY naming the
+ * member and cell. */
+int grhd_ensemble_advance(grhd_ensemble *ens, int steps, int use_graph,
+                          void *stream);
+/* Member time, CFL speed of its current state (0 before the first
+ * advance), Mdot of its last RHS, the Mdot time integral and the
+ * cumulative recovery counters. */
+int grhd_ensemble_member_info(grhd_ensemble *ens, int member, double *time,
+                              double *max_inverse_dt, double *mdot,
+                              double *mdot_integral, grhd_diagnostics *diag);
+int grhd_ensemble_reset_accretion(grhd_ensemble *ens);
+/* The member states were changed outside the ensemble: the next advance
+ * recomputes the CFL speed from them. */
+int grhd_ensemble_invalidate(grhd_ensemble *ens);
+/* Test hook: grid barriers wait for `extra_arrivals` more blocks than the
+ * grid has (none arrive, so every wait runs out after timeout_seconds and
+ * advance returns GRHD_ERR_CUDA); 0 and the default 4 s restore normal
+ * operation. */
+int grhd_ensemble_set_barrier_test(grhd_ensemble *ens,
+                                   unsigned int extra_arrivals,
+                                   double timeout_seconds);
+long long grhd_ensemble_launch_count(const grhd_ensemble *ens);
+
 #ifdef __cplusplus
 }
 #endif

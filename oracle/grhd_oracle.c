@@ -2272,8 +2272,8 @@ static double mi_bisect(const double *k, const orc_michel_config *c,
     return 0.5 * (lower + upper);
 }
 
-static double mi_density(const double *k, const orc_michel_config *c,
-                         double radius, int *ok)
+static double mi_density_sweep(const double *k, const orc_michel_config *c,
+                               double radius, int *ok)
 {
     if (fabs(radius - c->sonic_radius) < 1.0e-12)
         return c->sonic_density;
@@ -2321,6 +2321,34 @@ static double mi_density(const double *k, const orc_michel_config *c,
         sel_hi = first_hi;
     }
     return mi_bisect(k, c, radius, sel_lo, sel_hi, ok);
+}
+
+/* New (no reference counterpart): within MI_SONIC_BAND (relative) of the
+ * sonic radius the two density roots meet closer than one sample of the
+ * sweep, which then finds no sign change and the reference fails.  There
+ * the density is that of the branch the sweep selects on that side (the
+ * root above rho_s inside r_s, below it outside), from the quadratic
+ * through the sonic point and that branch's sweep solutions at
+ * r_s (1 +- MI_SONIC_BAND) and r_s (1 +- 2 MI_SONIC_BAND). */
+#define MI_SONIC_BAND 5.0e-3
+
+static double mi_density(const double *k, const orc_michel_config *c,
+                         double radius, int *ok)
+{
+    const double rho = mi_density_sweep(k, c, radius, ok);
+    const double x = radius / c->sonic_radius - 1.0;
+    if (*ok || !(fabs(x) < MI_SONIC_BAND))
+        return rho;
+    const double sg = x < 0.0 ? -1.0 : 1.0;
+    int o1 = 1, o2 = 1;
+    const double p1 = mi_density_sweep(
+        k, c, c->sonic_radius * (1.0 + sg * MI_SONIC_BAND), &o1);
+    const double p2 = mi_density_sweep(
+        k, c, c->sonic_radius * (1.0 + 2.0 * sg * MI_SONIC_BAND), &o2);
+    *ok = o1 && o2;
+    const double t = fabs(x) / MI_SONIC_BAND;
+    return 0.5 * (t - 1.0) * (t - 2.0) * c->sonic_density -
+           t * (t - 2.0) * p1 + 0.5 * t * (t - 1.0) * p2;
 }
 
 int orc_michel_point(const orc_params *p, const orc_michel_config *c,
