@@ -13,6 +13,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+// Pointwise functions of the FP64 path are also host-callable (the host
+// test of the adjoint's reverse-mode functions runs them on the CPU); the
+// FP32 overloads use device intrinsics and stay device-only.
+#define GRHD_HD __host__ __device__
+
 namespace grhd {
 
 // Symmetric 3x3 packing: 00 01 02 11 12 22.
@@ -27,25 +32,32 @@ __host__ __device__ constexpr int sym(int i, int j)
 // reference's expressions.  FP32: the SFU reciprocal / reciprocal square
 // root (a few ulp), which is what makes the FP32 path cheap.
 
-__device__ __forceinline__ double div_(double a, double b) { return a / b; }
+GRHD_HD __forceinline__ double div_(double a, double b) { return a / b; }
 __device__ __forceinline__ float div_(float a, float b)
 {
     return __fdividef(a, b);
 }
-__device__ __forceinline__ double rcp_(double a) { return 1.0 / a; }
+GRHD_HD __forceinline__ double rcp_(double a) { return 1.0 / a; }
 __device__ __forceinline__ float rcp_(float a) { return __fdividef(1.0f, a); }
-__device__ __forceinline__ double rsqrt_(double a) { return 1.0 / sqrt(a); }
+GRHD_HD __forceinline__ double rsqrt_(double a) { return 1.0 / sqrt(a); }
 __device__ __forceinline__ float rsqrt_(float a) { return rsqrtf(a); }
-__device__ __forceinline__ double sqrt_(double a) { return sqrt(a); }
+GRHD_HD __forceinline__ double sqrt_(double a) { return sqrt(a); }
 __device__ __forceinline__ float sqrt_(float a) { return sqrtf(a); }
-__device__ __forceinline__ double max_(double a, double b) { return fmax(a, b); }
+GRHD_HD __forceinline__ double max_(double a, double b) { return fmax(a, b); }
 __device__ __forceinline__ float max_(float a, float b) { return fmaxf(a, b); }
-__device__ __forceinline__ double min_(double a, double b) { return fmin(a, b); }
+GRHD_HD __forceinline__ double min_(double a, double b) { return fmin(a, b); }
 __device__ __forceinline__ float min_(float a, float b) { return fminf(a, b); }
-__device__ __forceinline__ double abs_(double a) { return fabs(a); }
+GRHD_HD __forceinline__ double abs_(double a) { return fabs(a); }
 __device__ __forceinline__ float abs_(float a) { return fabsf(a); }
 // the lapse (1 + 2H)^-1/2 of the Kerr-Schild metric
-__device__ __forceinline__ double lapse_rsqrt(double a) { return rsqrt(a); }
+GRHD_HD __forceinline__ double lapse_rsqrt(double a)
+{
+#ifdef __CUDA_ARCH__
+    return rsqrt(a);
+#else
+    return 1.0 / sqrt(a);
+#endif
+}
 __device__ __forceinline__ float lapse_rsqrt(float a) { return rsqrtf(a); }
 
 template <typename T> struct PrimT
@@ -124,7 +136,7 @@ struct Options
 // shift^i = 2H l^i/(1 + 2H l.l), gamma^ij by Sherman-Morrison
 // (KerrSchild.hpp:64-166; derivatives as get_KS_derivs, :171-242).
 template <typename T, bool FULL>
-__device__ __forceinline__ void ks_metric(T M, T a, T x, T y, T z,
+GRHD_HD __forceinline__ void ks_metric(T M, T a, T x, T y, T z,
                                           GeoT<T> &g, GeoFullT<T> *f)
 {
     const T a2 = a * a;
@@ -383,7 +395,7 @@ __device__ __forceinline__ void background_metric(const Background &bg,
 }
 
 template <typename A, typename B>
-__device__ __forceinline__ void convert_geo(const GeoT<A> &s, GeoT<B> &d)
+GRHD_HD __forceinline__ void convert_geo(const GeoT<A> &s, GeoT<B> &d)
 {
 #pragma unroll
     for (int q = 0; q < 6; ++q)
@@ -491,16 +503,26 @@ __device__ __forceinline__ void metric_T<float, true>(const Background &bg,
 // reference's separate multiply and subtract (no fused multiply-add), so
 // that positions -- and everything the time-difference volume source
 // amplifies -- match the reference bit for bit.
-__device__ __forceinline__ void cell_xyz(const Options &o, int i, int j,
+GRHD_HD __forceinline__ void cell_xyz(const Options &o, int i, int j,
                                          int k, double &x, double &y,
                                          double &z)
 {
+#ifdef __CUDA_ARCH__
     x = __dadd_rn(__dmul_rn(i + 0.5, o.dx), -o.center[0]);
     y = __dadd_rn(__dmul_rn(j + 0.5, o.dx), -o.center[1]);
     z = __dadd_rn(__dmul_rn(k + 0.5, o.dx), -o.center[2]);
+#else
+    // host: a separately rounded multiply and subtract (build the host
+    // code without floating-point contraction)
+    const volatile double px = (i + 0.5) * o.dx, py = (j + 0.5) * o.dx,
+                          pz = (k + 0.5) * o.dx;
+    x = px - o.center[0];
+    y = py - o.center[1];
+    z = pz - o.center[2];
+#endif
 }
 
-__device__ __forceinline__ bool excised(const Options &o, int i, int j, int k)
+GRHD_HD __forceinline__ bool excised(const Options &o, int i, int j, int k)
 {
     if (!(o.excision_radius > 0.0))
         return false;
@@ -522,7 +544,7 @@ __device__ __forceinline__ double pn_log_sqrt_det(double psi)
 // --------------------------------------------------------- Valencia, EOS
 
 template <typename T>
-__device__ __forceinline__ T vsq(const T v[3], const T gLL[6])
+GRHD_HD __forceinline__ T vsq(const T v[3], const T gLL[6])
 {
     return gLL[0] * v[0] * v[0] + gLL[3] * v[1] * v[1] + gLL[5] * v[2] * v[2] +
            T(2) * (gLL[1] * v[0] * v[1] + gLL[2] * v[0] * v[2] +
@@ -531,7 +553,7 @@ __device__ __forceinline__ T vsq(const T v[3], const T gLL[6])
 
 // compute_conserved, Valencia.hpp:55-73
 template <typename T>
-__device__ __forceinline__ ConsT<T> p2c(const PrimT<T> &pr, const T gLL[6])
+GRHD_HD __forceinline__ ConsT<T> p2c(const PrimT<T> &pr, const T gLL[6])
 {
     ConsT<T> c;
     const T vL0 = gLL[0] * pr.v[0] + gLL[1] * pr.v[1] + gLL[2] * pr.v[2];
@@ -550,7 +572,7 @@ __device__ __forceinline__ ConsT<T> p2c(const PrimT<T> &pr, const T gLL[6])
 }
 
 // detail::pressure_residual (+ derivative), Valencia.hpp:79-108.
-__device__ __forceinline__ double c2p_residual(double p, double D,
+GRHD_HD __forceinline__ double c2p_residual(double p, double D,
                                                double tau, double S2,
                                                double G, double Gfac,
                                                double vmax2, double *deriv)
@@ -569,7 +591,7 @@ __device__ __forceinline__ double c2p_residual(double p, double D,
     return D * W + Gfac * p * W2 - e;
 }
 
-__device__ __forceinline__ double c2p_S2(const Cons &c, const double gUU[6])
+GRHD_HD __forceinline__ double c2p_S2(const Cons &c, const double gUU[6])
 {
     return gUU[0] * c.S[0] * c.S[0] + gUU[3] * c.S[1] * c.S[1] +
            gUU[5] * c.S[2] * c.S[2] +
@@ -579,7 +601,7 @@ __device__ __forceinline__ double c2p_S2(const Cons &c, const double gUU[6])
 
 // The primitives of a converged pressure, Valencia.hpp:213-226; false when
 // the velocity reaches the cap.
-__device__ __forceinline__ bool c2p_finish(const Options &o, const Cons &c,
+GRHD_HD __forceinline__ bool c2p_finish(const Options &o, const Cons &c,
                                            const double gUU[6], double S2,
                                            double p, Prim &out)
 {
@@ -599,7 +621,7 @@ __device__ __forceinline__ bool c2p_finish(const Options &o, const Cons &c,
 }
 
 // recover_primitive, Valencia.hpp:116-228 (bounded loops throughout).
-__device__ __forceinline__ bool con2prim(const Options &o, const Cons &c,
+GRHD_HD __forceinline__ bool con2prim(const Options &o, const Cons &c,
                                          const double gUU[6], Prim &out,
                                          int *iters_out, double *resid_out)
 {
@@ -673,7 +695,7 @@ __device__ __forceinline__ bool con2prim(const Options &o, const Cons &c,
 // residual; falls back to the full bracketed solve when the guess is not
 // usable or a step leaves (p_floor, inf).  Converges to the same root to
 // the solver tolerance.
-__device__ __forceinline__ bool con2prim_warm(const Options &o, const Cons &c,
+GRHD_HD __forceinline__ bool con2prim_warm(const Options &o, const Cons &c,
                                               const double gUU[6],
                                               double p_guess, Prim &out)
 {
@@ -701,7 +723,7 @@ __device__ __forceinline__ bool con2prim_warm(const Options &o, const Cons &c,
 
 // enforce_primitive_floors, Atmosphere.hpp:24-46 (eps recomputed always)
 template <typename T>
-__device__ __forceinline__ void floors(const Options &o, PrimT<T> &pr,
+GRHD_HD __forceinline__ void floors(const Options &o, PrimT<T> &pr,
                                        const T gLL[6])
 {
     pr.rho = max_(pr.rho, T(o.rho_floor));
@@ -718,7 +740,7 @@ __device__ __forceinline__ void floors(const Options &o, PrimT<T> &pr,
 }
 
 // make_atmosphere_primitive, Atmosphere.hpp:48-60
-__device__ __forceinline__ Prim atmosphere(const Options &o)
+GRHD_HD __forceinline__ Prim atmosphere(const Options &o)
 {
     Prim pr;
     pr.rho = o.rho_floor;
@@ -730,7 +752,7 @@ __device__ __forceinline__ Prim atmosphere(const Options &o)
 
 // is_atmosphere_primitive, FArrayBoxFiniteVolume.hpp:118-126
 template <typename T>
-__device__ __forceinline__ bool is_atmo(const Options &o, const PrimT<T> &pr,
+GRHD_HD __forceinline__ bool is_atmo(const Options &o, const PrimT<T> &pr,
                                         double factor)
 {
     const double f = fmax(1.0, factor);
@@ -739,7 +761,7 @@ __device__ __forceinline__ bool is_atmo(const Options &o, const PrimT<T> &pr,
 
 // compute_flux, Valencia.hpp:230-259
 template <typename T>
-__device__ __forceinline__ ConsT<T> phys_flux(const PrimT<T> &pr,
+GRHD_HD __forceinline__ ConsT<T> phys_flux(const PrimT<T> &pr,
                                               const ConsT<T> &c, int d,
                                               T lapse, const T shift[3])
 {
@@ -756,7 +778,7 @@ __device__ __forceinline__ ConsT<T> phys_flux(const PrimT<T> &pr,
 
 // compute_characteristic_speeds (shifted), RiemannSolvers.hpp:23-67
 template <typename T>
-__device__ __forceinline__ void char_speeds(const Options &o,
+GRHD_HD __forceinline__ void char_speeds(const Options &o,
                                             const PrimT<T> &pr,
                                             const GeoT<T> &g, int d, T &lo,
                                             T &hi)
@@ -777,7 +799,7 @@ __device__ __forceinline__ void char_speeds(const Options &o,
 }
 
 // minmod / compute_limited_slope, Reconstruction.hpp:16-37
-template <typename T> __device__ __forceinline__ T minmod2(T l, T r)
+template <typename T> GRHD_HD __forceinline__ T minmod2(T l, T r)
 {
     if (l * r <= T(0))
         return T(0);
@@ -785,7 +807,7 @@ template <typename T> __device__ __forceinline__ T minmod2(T l, T r)
 }
 
 template <typename T>
-__device__ __forceinline__ T limited_slope(T l, T c, T r, T theta)
+GRHD_HD __forceinline__ T limited_slope(T l, T c, T r, T theta)
 {
     return minmod2(theta * (c - l), minmod2(T(0.5) * (r - l), theta * (r - c)));
 }
@@ -795,7 +817,7 @@ __device__ __forceinline__ T limited_slope(T l, T c, T r, T theta)
 // FArrayBoxFiniteVolume.hpp:194-216).  LL, L, R, RR are the cells
 // i-1, i, i+1, i+2 around face i+1/2.
 template <typename T>
-__device__ __forceinline__ ConsT<T> face_flux(const Options &o,
+GRHD_HD __forceinline__ ConsT<T> face_flux(const Options &o,
                                               const PVT<T> &LL,
                                               const PVT<T> &L,
                                               const PVT<T> &R,
@@ -859,7 +881,7 @@ __device__ __forceinline__ ConsT<T> face_flux(const Options &o,
 }
 
 template <typename T>
-__device__ __forceinline__ void average_geo(const GeoT<T> &a, const GeoT<T> &b,
+GRHD_HD __forceinline__ void average_geo(const GeoT<T> &a, const GeoT<T> &b,
                                             GeoT<T> &g)
 {
 #pragma unroll
@@ -876,7 +898,7 @@ __device__ __forceinline__ void average_geo(const GeoT<T> &a, const GeoT<T> &b,
 
 // compute_static_metric_source_terms, StaticMetric.hpp:193-275
 template <typename T>
-__device__ __forceinline__ ConsT<T> static_sources(const PrimT<T> &pr,
+GRHD_HD __forceinline__ ConsT<T> static_sources(const PrimT<T> &pr,
                                                    const ConsT<T> &c,
                                                    const GeoFullT<T> &f)
 {
@@ -940,7 +962,7 @@ __device__ __forceinline__ ConsT<T> static_sources(const PrimT<T> &pr,
 }
 
 template <typename A, typename B>
-__device__ __forceinline__ PrimT<B> convert_prim(const PrimT<A> &s)
+GRHD_HD __forceinline__ PrimT<B> convert_prim(const PrimT<A> &s)
 {
     PrimT<B> d;
     d.rho = B(s.rho);
@@ -953,7 +975,7 @@ __device__ __forceinline__ PrimT<B> convert_prim(const PrimT<A> &s)
 }
 
 template <typename A, typename B>
-__device__ __forceinline__ ConsT<B> convert_cons(const ConsT<A> &s)
+GRHD_HD __forceinline__ ConsT<B> convert_cons(const ConsT<A> &s)
 {
     ConsT<B> d;
     d.D = B(s.D);
