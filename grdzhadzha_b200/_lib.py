@@ -117,6 +117,17 @@ class Error(C.Structure):
 _P = C.POINTER
 _dp = _P(C.c_double)
 _vp = C.c_void_p
+class AdjointTorus(C.Structure):
+    """grhd_adjoint_torus: the eight differentiable parameters (amplitude,
+    entropy, spin, mode_amplitude[5]) and the fixed ones."""
+    _fields_ = [("amplitude", C.c_double), ("entropy", C.c_double),
+                ("spin", C.c_double), ("mode_amplitude", C.c_double * 5),
+                ("mode_phase", C.c_double * 5),
+                ("inner_radius", C.c_double),
+                ("pressure_max_radius", C.c_double),
+                ("max_velocity_squared", C.c_double)]
+
+
 SIGNATURES = {
     "grhd_abi_version": (C.c_int, []),
     "grhd_default_params": (None, [_P(Params)]),
@@ -181,6 +192,24 @@ SIGNATURES = {
     "grhd_ensemble_set_barrier_test": (C.c_int, [_vp, C.c_uint,
                                                  C.c_double]),
     "grhd_ensemble_launch_count": (C.c_longlong, [_vp]),
+    "grhd_default_adjoint_torus": (None, [_P(AdjointTorus)]),
+    "grhd_adjoint_unit_entropy": (C.c_int, [_P(Params), _P(AdjointTorus),
+                                            _dp]),
+    "grhd_adjoint_create": (C.c_int, [_P(Params), _P(Box), C.c_int, C.c_int,
+                                      C.c_double, _P(_vp)]),
+    "grhd_adjoint_destroy": (None, [_vp]),
+    "grhd_adjoint_last_error": (C.c_int, [_vp, _P(Error)]),
+    "grhd_adjoint_launch_count": (C.c_longlong, [_vp]),
+    "grhd_adjoint_initial_data": (C.c_int, [_vp, _P(AdjointTorus), _vp,
+                                            C.c_int64, _vp, C.c_int64, _vp]),
+    "grhd_adjoint_forward": (C.c_int, [_vp, _P(AdjointTorus), _dp, _vp]),
+    "grhd_adjoint_backward": (C.c_int, [_vp, _dp, _vp, C.c_int64, _vp]),
+    "grhd_adjoint_rhs_vjp": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_int64,
+                                       C.c_double, _vp, C.c_int64, _dp,
+                                       _vp]),
+    "grhd_adjoint_step_vjp": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_int64,
+                                        C.c_double, _vp, C.c_int64, _dp,
+                                        _vp]),
 }
 
 _lib = None

@@ -754,3 +754,268 @@ GRHD_HD inline Dual sqrt_det(const Dual g[6])
 
 } // namespace adj
 } // namespace grhd
+
+namespace grhd {
+namespace adj {
+
+// Whether the floors or atmosphere changed the primitives
+// (primitive_differs, FArrayBoxFiniteVolume.hpp:704-711).
+GRHD_HD inline bool differs(const Prim &a, const Prim &b)
+{
+    return a.rho != b.rho || a.eps != b.eps || a.p != b.p ||
+           a.v[0] != b.v[0] || a.v[1] != b.v[1] || a.v[2] != b.v[2];
+}
+
+// Reverse of the post-update recovery of one cell
+// (recover_primitives_and_apply_atmosphere_from_fixed_background,
+// FixedBGFArrayBoxFiniteVolume.hpp:60-110) as recorded by the forward
+// sweep: branch 0 kept the updated state Y, 1 replaced it by p2c of the
+// floored con2prim result (converged pressure pY), 2 by the atmosphere.
+GRHD_HD inline ConsBar recovery_rev(const Options &o, const Cons &Y, int br,
+                                    double pY, const Geo &g,
+                                    const ConsBar &Ub, GeoBar &gb)
+{
+    if (br == 0)
+        return Ub;
+    ConsBar Yb = zero_cons_bar();
+    if (br != 1)
+        return Yb;
+    const Prim pr = c2p_at(o, Y, g.gUU, pY);
+    Prim fl = pr;
+    floors(o, fl, g.gLL);
+    PrimBar flb = zero_prim_bar(), prb = zero_prim_bar();
+    p2c_rev(fl, g.gLL, Ub, flb, gb.gLL);
+    floors_rev(o, pr, g.gLL, flb, prb, gb.gLL);
+    con2prim_rev(o, Y, g.gUU, pY, prb, Yb, gb.gUU);
+    return Yb;
+}
+
+// ----------------------------------------------- torus initial data
+// The constant-specific-angular-momentum torus of FixedBGTorus.hpp
+// (fixed_bg_torus_primitive, :333-374) with eight parameters: an amplitude
+// A scaling the equilibrium density and pressure (the test-fluid
+// equilibrium is invariant under it), the polytropic constant K, the spin
+// a of the Kerr-Schild hole (metric and torus), and five azimuthal density
+// modes rho *= 1 + sum_m eps_m cos(m phi + phase_m).  Templated so that
+// the same code gives the state (double) and its derivative along one
+// parameter (Dual).
+
+template <typename T> struct TorusThetaT
+{
+    T A, K, a, eps[5];
+    T ell, W_in; // angular momentum and surface potential of spin a
+};
+
+template <typename T>
+GRHD_HD inline bool torus_potential_T(T x, T y, T ell, const GeoT<T> &g,
+                                      double vmax2, T &W)
+{
+    const T b[3] = {-y, x, T(0.0)};
+    T gpp = T(0.0), gtp = T(0.0), bb = T(0.0);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            gpp += g.gLL[sym(i, j)] * b[i] * b[j];
+    for (int i = 0; i < 3; ++i)
+    {
+        T sL = T(0.0);
+        for (int j = 0; j < 3; ++j)
+            sL += g.gLL[sym(i, j)] * g.shift[j];
+        gtp += sL * b[i];
+        bb += sL * g.shift[i];
+    }
+    const T gtt = bb - g.lapse * g.lapse;
+    const T den = ell * gtp + gpp;
+    if (fabs(val(den)) < 1.0e-300)
+        return false;
+    const T om = -(ell * gtt + gtp) / den;
+    T v[3];
+    for (int i = 0; i < 3; ++i)
+        v[i] = (om * b[i] + g.shift[i]) / g.lapse;
+    const T v2 = vsq(v, g.gLL);
+    if (val(v2) >= vmax2 || val(v2) >= 1.0)
+        return false;
+    const T norm = -gtt - T(2.0) * om * gtp - om * om * gpp;
+    if (val(norm) <= 0.0)
+        return false;
+    const T mut = -(gtt + om * gtp) / sqrt_(norm);
+    if (val(mut) <= 0.0)
+        return false;
+    W = log_(mut);
+    return true;
+}
+
+template <typename T>
+GRHD_HD inline void torus_velocity_T(T x, T y, T ell, const GeoT<T> &g,
+                                     T v[3])
+{
+    const T b[3] = {-y, x, T(0.0)};
+    T gpp = T(0.0), gtp = T(0.0), bb = T(0.0);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            gpp += g.gLL[sym(i, j)] * b[i] * b[j];
+    for (int i = 0; i < 3; ++i)
+    {
+        T sL = T(0.0);
+        for (int j = 0; j < 3; ++j)
+            sL += g.gLL[sym(i, j)] * g.shift[j];
+        gtp += sL * b[i];
+        bb += sL * g.shift[i];
+    }
+    const T gtt = bb - g.lapse * g.lapse;
+    const T om = -(ell * gtt + gtp) / (ell * gtp + gpp);
+    for (int i = 0; i < 3; ++i)
+        v[i] = (om * b[i] + g.shift[i]) / g.lapse;
+}
+
+// Primitives and conserved variables of one cell centre (x, y, z) relative
+// to the hole.  r_in: the torus's inner edge (cylindrical radius below
+// which the atmosphere is kept, as the reference's fill does); vmax2: the
+// torus configuration's velocity cap of the potential.
+template <typename T>
+GRHD_HD inline ConsT<T> torus_cell_T(const Options &o, double M,
+                                     const TorusThetaT<T> &th,
+                                     const double phase[5], double r_in,
+                                     double vmax2, double x, double y,
+                                     double z, PrimT<T> &pr)
+{
+    GeoT<T> g;
+    ks_metric<T, false>(T(M), th.a, T(x), T(y), T(z), g, nullptr);
+    const double G = o.G;
+    pr.rho = T(o.rho_floor);
+    pr.p = T(o.p_floor);
+    pr.v[0] = pr.v[1] = pr.v[2] = T(0.0);
+    pr.eps = pr.p / (T(G - 1.0) * pr.rho);
+    if (sqrt(x * x + y * y) >= r_in)
+    {
+        T W;
+        if (torus_potential_T(T(x), T(y), th.ell, g, vmax2, W))
+        {
+            const T h = exp_(th.W_in - W);
+            if (val(h) > 1.0)
+            {
+                const T rho_eq =
+                    pow_((h - T(1.0)) * T(G - 1.0) / (T(G) * th.K),
+                         1.0 / (G - 1.0));
+                const T p_eq = th.K * pow_(rho_eq, G);
+                const double phi = atan2(y, x);
+                T pert = T(1.0);
+                for (int m = 0; m < 5; ++m)
+                    pert += th.eps[m] * cos((m + 1) * phi + phase[m]);
+                pr.rho = th.A * rho_eq * pert;
+                pr.p = th.A * p_eq;
+                pr.eps = pr.p / (T(G - 1.0) * pr.rho);
+                torus_velocity_T(T(x), T(y), th.ell, g, pr.v);
+            }
+        }
+    }
+    floors(o, pr, g.gLL);
+    return p2c(pr, g.gLL);
+}
+
+// d W / d R at R on the x axis by the centred difference of
+// fixed_bg_torus_radial_potential_derivative (FixedBGTorus.hpp:200-216);
+// false when the potential is not finite there.
+template <typename T>
+GRHD_HD inline bool torus_dWdr_T(double M, T a, T ell, double R,
+                                 double vmax2, T &out)
+{
+    const double dr = fmax(1.0e-3 * R, 1.0e-4);
+    const double rm = fmax(R - dr, 1.0e-6);
+    GeoT<T> gp, gm;
+    ks_metric<T, false>(T(M), a, T(R + dr), T(0.0), T(0.0), gp, nullptr);
+    ks_metric<T, false>(T(M), a, T(rm), T(0.0), T(0.0), gm, nullptr);
+    T wp, wm;
+    if (!torus_potential_T(T(R + dr), T(0.0), ell, gp, vmax2, wp) ||
+        !torus_potential_T(T(rm), T(0.0), ell, gm, vmax2, wm))
+        return false;
+    out = (wp - wm) / T(R + dr - rm);
+    return true;
+}
+
+// Torus constants of spin a with their spin derivatives: the angular
+// momentum ell whose potential is stationary at the pressure maximum
+// (fixed_bg_torus_pressure_max_specific_angular_momentum,
+// FixedBGTorus.hpp:218-281: a scan of 120 values in [0.25, 4] x the
+// Schwarzschild guess, then bisection to |dW/dR| < 1e-13), the surface
+// potential W_in at the inner edge, and the polytropic constant K that
+// gives density 1 at the pressure maximum.  d ell / d a follows from the
+// implicit function theorem on dW/dR(ell, a) = 0.  False when no torus
+// exists for these radii.
+struct TorusSetup
+{
+    double ell, dell_da, W_in, dWin_da, K_unit;
+};
+
+GRHD_HD inline bool torus_setup(double M, double a, double r_in,
+                                double r_max, double vmax2, double G,
+                                TorusSetup &out)
+{
+    if (r_max <= 3.0 * M)
+        return false;
+    const double guess = sqrt(M * r_max) / (1.0 - 2.0 * M / r_max);
+    double ell = guess;
+    double prev_ell = 0.25 * guess, prev_d = 0.0;
+    bool prev_ok = torus_dWdr_T<double>(M, a, prev_ell, r_max, vmax2, prev_d);
+    for (int s = 1; s <= 120; ++s)
+    {
+        const double e = guess * (0.25 + (double)s / 120.0 * 3.75);
+        double d;
+        if (!torus_dWdr_T<double>(M, a, e, r_max, vmax2, d))
+            continue;
+        if (prev_ok && prev_d * d <= 0.0)
+        {
+            double lo = prev_ell, hi = e, flo = prev_d;
+            ell = 0.5 * (lo + hi);
+            for (int it = 0; it < 80; ++it)
+            {
+                const double mid = 0.5 * (lo + hi);
+                double fm;
+                if (!torus_dWdr_T<double>(M, a, mid, r_max, vmax2, fm))
+                    break;
+                ell = mid;
+                if (fabs(fm) < 1.0e-13)
+                    break;
+                if (flo * fm <= 0.0)
+                    hi = mid;
+                else
+                {
+                    lo = mid;
+                    flo = fm;
+                }
+                ell = 0.5 * (lo + hi);
+            }
+            break;
+        }
+        prev_ell = e;
+        prev_d = d;
+        prev_ok = true;
+    }
+    Dual ge, ga;
+    if (!torus_dWdr_T<Dual>(M, Dual(a), Dual(ell, 1.0), r_max, vmax2, ge) ||
+        !torus_dWdr_T<Dual>(M, Dual(a, 1.0), Dual(ell), r_max, vmax2, ga))
+        return false;
+    out.ell = ell;
+    out.dell_da = -ga.d / ge.d;
+    GeoT<Dual> g;
+    ks_metric<Dual, false>(Dual(M), Dual(a, 1.0), Dual(r_in), Dual(0.0),
+                           Dual(0.0), g, nullptr);
+    Dual W;
+    if (!torus_potential_T<Dual>(Dual(r_in), Dual(0.0),
+                                 Dual(ell, out.dell_da), g, vmax2, W))
+        return false;
+    out.W_in = W.v;
+    out.dWin_da = W.d;
+    Geo gc;
+    ks_metric<double, false>(M, a, r_max, 0.0, 0.0, gc, nullptr);
+    double Wc;
+    if (!torus_potential_T<double>(r_max, 0.0, ell, gc, vmax2, Wc))
+        return false;
+    const double hc = exp(out.W_in - Wc);
+    if (!(hc > 1.0))
+        return false;
+    out.K_unit = (hc - 1.0) * (G - 1.0) / G;
+    return true;
+}
+
+} // namespace adj
+} // namespace grhd

@@ -117,3 +117,39 @@ def batched_ensemble(count=96, sizes=(32, 48, 64, 96, 128), seed=SEED + 3,
         members.append((op, lv))
         specs.append(spec)
     return members, specs
+
+
+def adjoint_torus(n=128, half_width=20.0, steps=400, checkpoint_every=25,
+                  spin=0.7, gamma=5.0 / 3.0, inner_radius=3.5,
+                  pressure_max_radius=6.0, accretion_radius=2.5, cfl=0.25,
+                  device="cuda"):
+    """The adjoint workload: a constant-angular-momentum torus around a
+    Kerr-Schild hole (M = 1, spin 0.7) on an n^3 grid over
+    [-half_width, half_width]^3, inner edge 3.5, pressure maximum 6 (close
+    enough that its inner edge spills through r = 2.5 within the run),
+    Gamma 5/3, density 1 at the pressure maximum, five azimuthal density
+    modes of amplitudes 1e-2 .. 2e-3 with fixed phases, atmosphere
+    1e-10 / 1e-12 / v^2 cap 0.8, recovery v^2 cap 0.9, MUSCL-MC + HLLE,
+    excision r < 1.5; J = integral of the accretion rate through r = 2.5
+    over `steps` RK4 steps of the fixed size cfl / (max inverse dt of the
+    initial state).  Returns (operator, adjoint)."""
+    from .adjoint import TorusAccretionAdjoint, default_torus
+    nn = (n, n, n) if isinstance(n, int) else tuple(n)
+    dx = 2.0 * half_width / nn[0]
+    c = tuple(0.5 * nn[d] * dx for d in range(3))
+    op = TimeDependentFixedBGLevelDataFiniteVolumeOperator(
+        IdealGasEOS(gamma), KerrSchild(mass=1.0, spin=spin, dx=dx), dx, c,
+        AtmosphereOptions(1e-10, 1e-12, 0.8), 2.0, True,
+        RecoveryOptions(80, 1e-12, 1e-12, 0.9), True, False, 1e-3, 1.5,
+        accretion_radius, "fp64")
+    lv = LevelBox.cube(nn, device=device)
+    torus = default_torus(spin=spin, inner_radius=inner_radius,
+                          pressure_max_radius=pressure_max_radius)
+    # the step size: CFL of the initial state, computed by a one-step
+    # adjoint object (no tape beyond one step)
+    probe = TorusAccretionAdjoint(op, lv, 1, 1, 1.0, torus)
+    probe.initial_state(level=lv)
+    dt = cfl / op.compute_max_inverse_dt(lv)
+    del probe
+    adj = TorusAccretionAdjoint(op, lv, steps, checkpoint_every, dt, torus)
+    return op, adj

@@ -434,6 +434,87 @@ int grhd_ensemble_set_barrier_test(grhd_ensemble *ens,
                                    double timeout_seconds);
 long long grhd_ensemble_launch_count(const grhd_ensemble *ens);
 
+
+/* ---- discrete adjoint (new; no reference counterpart) ----
+ * Reverse-mode kernels of the FP64 Kerr-Schild operator (one box covering
+ * the domain, ghost width 2): the RHS, one RK4 step with its post-update
+ * recoveries, and a checkpointed forward/backward pair for
+ *   J = integral over the run of the rest-mass accretion rate through the
+ *       sphere r < params.accretion_radius (grhd_accretion's quantity),
+ * as a function of the eight parameters of a torus initial state.  The
+ * backward replays the MUSCL limiter branches recorded by the forward,
+ * runs the HLLE flux in reverse, differentiates con2prim by the implicit
+ * function theorem at the converged pressure, and gets spin derivatives
+ * of the analytic metric in dual numbers.  The step size is fixed (dt), so
+ * J is differentiated along a fixed step sequence. */
+typedef struct grhd_adjoint grhd_adjoint;
+
+/* Initial data: the constant-angular-momentum torus of
+ * FixedBGTorus.hpp:291-409 (inner edge, pressure maximum, velocity cap of
+ * the potential) with density and pressure scaled by `amplitude`,
+ * polytropic constant `entropy` (<= 0: the value giving density 1 at the
+ * pressure maximum), Kerr-Schild spin `spin` (also the operator's), and
+ * density modes rho *= 1 + sum_m mode_amplitude[m-1] cos(m phi +
+ * mode_phase[m-1]), m = 1..5.  The gradient is ordered
+ *   [amplitude, entropy, spin, mode_amplitude[0..4]]. */
+typedef struct grhd_adjoint_torus
+{
+    double amplitude, entropy, spin;
+    double mode_amplitude[5], mode_phase[5];
+    double inner_radius, pressure_max_radius, max_velocity_squared;
+} grhd_adjoint_torus;
+
+void grhd_default_adjoint_torus(grhd_adjoint_torus *torus);
+/* The entropy (polytropic constant) that gives density 1 at the pressure
+ * maximum for these radii and spin. */
+int grhd_adjoint_unit_entropy(const grhd_params *params,
+                              const grhd_adjoint_torus *torus, double *K);
+/* params: FP64 Kerr-Schild operator (its spin is replaced by the torus
+ * spin of each forward); box == domain.  Allocates the tape of
+ * `checkpoint_every` steps (about 1.6 KB per cell per step) and one
+ * checkpoint per segment.  On error *out is still set. */
+int grhd_adjoint_create(const grhd_params *params, const grhd_box *box,
+                        int steps, int checkpoint_every, double dt,
+                        grhd_adjoint **out);
+void grhd_adjoint_destroy(grhd_adjoint *adj);
+int grhd_adjoint_last_error(const grhd_adjoint *adj, grhd_error *out);
+long long grhd_adjoint_launch_count(const grhd_adjoint *adj);
+/* The initial state of `torus` (11 components over the ghosted box, may be
+ * NULL) and/or its tangents dU0/dtheta_k (8 x 5 components over the
+ * interior, component (k, c) at tangent + (5k + c) * stride; may be
+ * NULL).  Device pointers; synchronous. */
+int grhd_adjoint_initial_data(grhd_adjoint *adj,
+                              const grhd_adjoint_torus *torus, double *state,
+                              int64_t state_cs, double *tangent,
+                              int64_t tangent_comp_stride, void *stream);
+/* Forward: the initial state of `torus`, `steps` RK4 steps of size dt,
+ * checkpoints every `checkpoint_every` steps; *J receives J.
+ * Synchronous. */
+int grhd_adjoint_forward(grhd_adjoint *adj, const grhd_adjoint_torus *torus,
+                         double *J, void *stream);
+/* Backward of the last forward: grad[8] = dJ/dtheta; lambda0 (device, 5
+ * components over the interior, may be NULL) = dJ/dU0.  Synchronous. */
+int grhd_adjoint_backward(grhd_adjoint *adj, double grad[8], double *lambda0,
+                          int64_t lambda_comp_stride, void *stream);
+/* Vector-Jacobian product of one RHS evaluation (grhd_compute_rhs of the
+ * FP64 operator with the adjoint's parameters, spin = params.ks_spin):
+ * state_bar = (dRHS/dU)^T rhs_bar + mdot_bar dMdot/dU over the interior
+ * conserved variables; *spin_bar = the same product's spin derivative.
+ * Fills the physical ghosts of `state` as compute_rhs does. */
+int grhd_adjoint_rhs_vjp(grhd_adjoint *adj, double *state, int64_t state_cs,
+                         const double *rhs_bar, int64_t rhs_bar_cs,
+                         double mdot_bar, double *state_bar,
+                         int64_t state_bar_cs, double *spin_bar,
+                         void *stream);
+/* Vector-Jacobian product of one RK4 step of size dt (grhd_advance_rk4):
+ * given the adjoint of U^{n+1} and the weight of the step's accretion
+ * integral, the adjoint of U^n and the spin derivative. */
+int grhd_adjoint_step_vjp(grhd_adjoint *adj, const double *state,
+                          int64_t state_cs, const double *state_bar_next,
+                          int64_t next_cs, double mdot_integral_bar,
+                          double *state_bar, int64_t state_bar_cs,
+                          double *spin_bar, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

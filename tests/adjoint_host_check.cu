@@ -531,6 +531,153 @@ static void check_sources()
     }
 }
 
+// ------------------------------------------------- post-update recovery
+static Cons recover_fwd(const Options &o, const Cons &Y, const Geo &g, int &br)
+{
+    Prim pr;
+    if (!con2prim(o, Y, g.gUU, pr, nullptr, nullptr))
+    {
+        br = 2;
+        return p2c(atmosphere(o), g.gLL);
+    }
+    Prim fl = pr;
+    floors(o, fl, g.gLL);
+    br = differs(pr, fl) ? 1 : 0;
+    return br ? p2c(fl, g.gLL) : Y;
+}
+
+static void check_recovery()
+{
+    Options o = opts();
+    o.atmo_vmax2 = 0.3; // so that the velocity cap resets some cells
+    int n1 = 0;
+    for (int t = 0; t < 40; ++t)
+    {
+        const double x = U(-8, 8), y = U(-8, 8), z = U(-8, 8);
+        const Geo g = geo_at(x, y, z);
+        const Prim p = rand_prim(0.5);
+        const Cons Y = p2c(p, g.gLL);
+        int br;
+        recover_fwd(o, Y, g, br);
+        Prim pr;
+        con2prim(o, Y, g.gUU, pr, nullptr, nullptr);
+        const ConsBar Ub = rand_cbar();
+        GeoBar gb;
+        zero(gb);
+        const ConsBar Yb = recovery_rev(o, Y, br, pr.p, g, Ub, gb);
+        if (br == 1)
+            ++n1;
+        const double ybv[5] = {Yb.D, Yb.S[0], Yb.S[1], Yb.S[2], Yb.tau};
+        for (int k = 0; k < 5; ++k)
+        {
+            Cons a = Y, m = Y;
+            double *pa = k == 0 ? &a.D : k == 4 ? &a.tau : &a.S[k - 1];
+            double *pm = k == 0 ? &m.D : k == 4 ? &m.tau : &m.S[k - 1];
+            const double h = 1e-6 * fmax(1e-2, fabs(*pa));
+            *pa += h;
+            *pm -= h;
+            int ba, bm;
+            const double fd = (dotc(Ub, recover_fwd(o, a, g, ba)) -
+                               dotc(Ub, recover_fwd(o, m, g, bm))) / (2 * h);
+            if (ba != br || bm != br)
+                continue;
+            report("recovery d/dY", ybv[k], fd, 1.0 + fabs(fd), 1e-5);
+        }
+    }
+    if (n1 < 5)
+    {
+        printf("FAIL recovery: only %d reset samples\n", n1);
+        ++g_fail;
+    }
+}
+
+// --------------------------------------------------- torus initial data
+static void check_torus()
+{
+    Options o = opts();
+    const double M = 1.0, r_in = 3.0, r_max = 5.0, vmax2 = 0.8;
+    const double phase[5] = {0.3, 1.1, 2.0, 4.0, 5.5};
+    auto theta_at = [&](const double th[8], TorusThetaT<double> &T,
+                        TorusSetup &S) {
+        if (!torus_setup(M, th[2], r_in, r_max, vmax2, o.G, S))
+            return false;
+        T.A = th[0];
+        T.K = th[1];
+        T.a = th[2];
+        for (int m = 0; m < 5; ++m)
+            T.eps[m] = th[3 + m];
+        T.ell = S.ell;
+        T.W_in = S.W_in;
+        return true;
+    };
+    double th0[8] = {1.0, 0.0, 0.7, 0.01, 0.008, 0.006, 0.004, 0.002};
+    TorusSetup S0;
+    if (!torus_setup(M, th0[2], r_in, r_max, vmax2, o.G, S0))
+    {
+        printf("FAIL torus setup\n");
+        ++g_fail;
+        return;
+    }
+    th0[1] = S0.K_unit;
+    int checked = 0;
+    for (int t = 0; t < 400 && checked < 40; ++t)
+    {
+        const double R = U(3.2, 8.0), ph = U(0, 6.283), z = U(-1.0, 1.0);
+        const double x = R * cos(ph), y = R * sin(ph);
+        TorusThetaT<double> T0;
+        TorusSetup S;
+        theta_at(th0, T0, S);
+        PrimT<double> p0;
+        torus_cell_T<double>(o, M, T0, phase, r_in, vmax2, x, y, z, p0);
+        if (!(p0.rho > 1e-6))
+            continue; // atmosphere: parameter independent
+        ++checked;
+        const ConsBar w = rand_cbar();
+        for (int k = 0; k < 8; ++k)
+        {
+            TorusThetaT<Dual> TD;
+            TD.A = Dual(th0[0], k == 0);
+            TD.K = Dual(th0[1], k == 1);
+            TD.a = Dual(th0[2], k == 2);
+            for (int m = 0; m < 5; ++m)
+                TD.eps[m] = Dual(th0[3 + m], k == 3 + m);
+            TD.ell = Dual(S0.ell, k == 2 ? S0.dell_da : 0.0);
+            TD.W_in = Dual(S0.W_in, k == 2 ? S0.dWin_da : 0.0);
+            PrimT<Dual> pd;
+            const ConsT<Dual> cd =
+                torus_cell_T<Dual>(o, M, TD, phase, r_in, vmax2, x, y, z, pd);
+            const double got = w.D * cd.D.d + w.tau * cd.tau.d +
+                               w.S[0] * cd.S[0].d + w.S[1] * cd.S[1].d +
+                               w.S[2] * cd.S[2].d;
+            const double h = 1e-6 * fmax(0.1, fabs(th0[k]));
+            double tp[8], tm[8];
+            for (int q = 0; q < 8; ++q)
+                tp[q] = tm[q] = th0[q];
+            tp[k] += h;
+            tm[k] -= h;
+            TorusThetaT<double> Tp, Tm;
+            TorusSetup Sp, Sm;
+            theta_at(tp, Tp, Sp);
+            theta_at(tm, Tm, Sm);
+            PrimT<double> pp, pm;
+            const Cons cp =
+                torus_cell_T<double>(o, M, Tp, phase, r_in, vmax2, x, y, z, pp);
+            const Cons cm =
+                torus_cell_T<double>(o, M, Tm, phase, r_in, vmax2, x, y, z, pm);
+            const double fd = (dotc(w, cp) - dotc(w, cm)) / (2 * h);
+            char lbl[64];
+            snprintf(lbl, sizeof lbl, "torus d/dtheta[%d]", k);
+            report(lbl, got, fd,
+                   1e-3 + fabs(fd), 1e-5);
+        }
+    }
+    if (checked < 20)
+    {
+        printf("FAIL torus: only %d torus cells sampled\n", checked);
+        ++g_fail;
+    }
+}
+
 int main()
 {
     check_p2c();
@@ -539,6 +686,8 @@ int main()
     check_face();
     check_con2prim();
     check_sources();
+    check_recovery();
+    check_torus();
     printf("%s: %d failures\n", g_fail ? "FAILED" : "PASSED", g_fail);
     return g_fail ? 1 : 0;
 }
