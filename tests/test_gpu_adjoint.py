@@ -144,9 +144,13 @@ def test_forward_sweep_matches_operator_run():
 
 def test_gradient_matches_central_differences():
     """J through the sphere r = 5, inside the torus body, where it depends
-    smoothly on every parameter within a few steps."""
+    on every parameter from the first step.  Four steps (two checkpoint
+    segments): over longer runs the trajectory crosses limiter, floor and
+    HLLE switches within h = 1e-6 of the parameters, J(theta) is only
+    piecewise smooth at that scale and central differences stop measuring
+    a derivative (at 24^3 they scatter by 1e-4 after 12 steps)."""
     from grdzhadzha_b200.adjoint import THETA_NAMES, AccretionIntegral
-    steps, every = 12, 5
+    steps, every = 4, 3
     op, adj = _workload(steps=steps, every=every, accretion_radius=5.0)
     theta = torch.tensor(adj.theta(), dtype=torch.float64,
                          requires_grad=True)
