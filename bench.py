@@ -339,6 +339,70 @@ def run_ensemble(count, steps, warmup, hbm_peak):
     return out
 
 
+# ------------------------------------------------------ discrete adjoint
+
+
+def run_adjoint(n, steps, every, fd_steps, hbm_peak):
+    """The adjoint workload (Kerr-Schild torus a = 0.7, n^3 on [-20, 20]^3,
+    J = integral of the accretion rate through r = 2.5 over `steps` RK4
+    steps, checkpoint every `every`): forward and backward sweep timed with
+    CUDA events, their ratio, the gradient; then, on a run of `fd_steps`
+    steps with the sphere r = 5 inside the torus body (within the horizon
+    over which J is smooth at the 1e-6 scale), the gradient against central
+    differences with h = 1e-6 relative."""
+    import torch
+    from grdzhadzha_b200 import workloads as W
+    from grdzhadzha_b200.adjoint import THETA_NAMES
+    out = {"config": {"workload": f"adjoint_kerr_schild_torus_a0.7_{n}^3",
+                      "steps": steps, "checkpoint_every": every,
+                      "domain": [-20.0, 20.0], "accretion_radius": 2.5,
+                      "torus": {"inner_radius": 3.5,
+                                "pressure_max_radius": 6.0},
+                      "parameters": list(THETA_NAMES), "dtype": "f64"}}
+    op, adj = W.adjoint_torus(n=n, steps=steps, checkpoint_every=every)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    adj.forward()  # warm-up (allocation-free afterwards)
+    torch.cuda.synchronize()
+    l0 = adj.launch_count()
+    ev[0].record()
+    J = adj.forward()
+    ev[1].record()
+    grad = adj.backward()
+    ev[2].record()
+    torch.cuda.synchronize()
+    fwd, bwd = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    cells = n ** 3
+    out.update({
+        "J": J, "gradient": dict(zip(THETA_NAMES, grad)), "dt": adj.dt,
+        "forward_ms": fwd, "backward_ms": bwd,
+        "backward_over_forward": bwd / fwd,
+        "forward_cell_updates_per_s": cells * steps / (fwd / 1e3),
+        "gpu_launches": adj.launch_count() - l0})
+    del adj, op
+    torch.cuda.empty_cache()
+    if fd_steps > 0:
+        op, adj = W.adjoint_torus(n=n, steps=fd_steps,
+                                  checkpoint_every=min(every, fd_steps),
+                                  accretion_radius=5.0)
+        adj.forward()
+        g = adj.backward()
+        base = adj.theta()
+        rows = {}
+        for k, name in enumerate(THETA_NAMES):
+            h = 1e-6 * max(abs(base[k]), 0.1)
+            tp, tm = list(base), list(base)
+            tp[k] += h
+            tm[k] -= h
+            fd = (adj.forward(tp) - adj.forward(tm)) / (2 * h)
+            rows[name] = {"adjoint": g[k], "central_difference": fd,
+                          "rel_err": abs(g[k] - fd) / max(abs(fd), 1e-300)}
+        out["fd_check"] = {"steps": fd_steps, "accretion_radius": 5.0,
+                           "h_rel": 1e-6, "rows": rows}
+        del adj, op
+        torch.cuda.empty_cache()
+    return out
+
+
 # ------------------------------------------------------------ CPU oracle
 
 
@@ -429,6 +493,13 @@ def main():
                     help="skip the mixed 256^3 and batched-ensemble legs")
     ap.add_argument("--ensemble-count", type=int, default=96)
     ap.add_argument("--ensemble-steps", type=int, default=100)
+    ap.add_argument("--adjoint-n", type=int, default=128)
+    ap.add_argument("--adjoint-steps", type=int, default=400)
+    ap.add_argument("--adjoint-every", type=int, default=25)
+    ap.add_argument("--adjoint-fd-steps", type=int, default=25)
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="run only the adjoint leg and print its JSON")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -463,6 +534,14 @@ def main():
                     "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
         print(json.dumps(line), flush=True)
+        return
+
+    if args.adjoint_only:
+        import torch
+        torch.cuda.set_device(local_rank)
+        print(json.dumps({"adjoint": run_adjoint(
+            args.adjoint_n, args.adjoint_steps, args.adjoint_every,
+            args.adjoint_fd_steps, None)}), flush=True)
         return
 
     if world > 1:
@@ -502,6 +581,10 @@ def main():
         ens["mixed"]["speedup_vs_fp64_plain"] = (
             ens["mixed"]["value"] / res["value"])
         variants["batched_ensemble"] = ens
+        if not args.no_adjoint:
+            variants["adjoint"] = run_adjoint(
+                args.adjoint_n, args.adjoint_steps, args.adjoint_every,
+                args.adjoint_fd_steps, hbm_peak)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = host_threads()
