@@ -95,7 +95,8 @@ __global__ void __launch_bounds__(256)
                         t);
 }
 
-__global__ void __launch_bounds__(kAdjThreads)
+// three resident blocks per SM (168 registers, small spills)
+__global__ void __launch_bounds__(kAdjThreads, 3)
     k_adj_faces(AdjRhs A, int d, double *slot)
 {
     int n[3] = {A.b.in[0], A.b.in[1], A.b.in[2]};

@@ -699,6 +699,19 @@ GRHD_HD __forceinline__ bool con2prim_warm(const Options &o, const Cons &c,
                                               const double gUU[6],
                                               double p_guess, Prim &out)
 {
+    if (c.D > 0.0 && !(p_guess > o.rec_pfloor))
+    {
+        // a guess at (or rounded below) the recovery floor: the full solve
+        // returns the floor itself when the residual there is within
+        // tolerance; test that first
+        const double G = o.G;
+        const double S2 = c2p_S2(c, gUU);
+        const double r = c2p_residual(o.rec_pfloor, c.D, c.tau, S2, G,
+                                      G / (G - 1.0), o.rec_vmax2, nullptr);
+        if (fabs(r) <= o.rec_tol)
+            return c2p_finish(o, c, gUU, S2, o.rec_pfloor, out) ||
+                   con2prim(o, c, gUU, out, nullptr, nullptr);
+    }
     if (c.D > 0.0 && p_guess > o.rec_pfloor && isfinite(p_guess))
     {
         const double G = o.G;

@@ -1101,11 +1101,26 @@ stage_item(const double *un, int64_t ucs, const double *us, int64_t tcs,
         if (prep || cfl)
         {
             // con2prim of the state just written (unchanged cells:
-            // the same solve on the same input gives pr again)
+            // the same solve on the same input gives pr again).  The mixed
+            // path takes the primitives of a cell reset to the atmosphere
+            // or to the density / pressure floors as they are: con2prim of
+            // their p2c returns them to within its residual tolerance, far
+            // below the FP32 rounding of the primitive cache.  The FP64
+            // path re-solves, as the reference's next con2prim does.
             Prim pn = pr;
             bool okn = ok;
             if (reset)
-                okn = cell_con2prim(o, c, f.g, stored.p, pn);
+            {
+                if (mixed && (!ok || (stored.v[0] == pr.v[0] &&
+                                      stored.v[1] == pr.v[1] &&
+                                      stored.v[2] == pr.v[2])))
+                {
+                    pn = stored;
+                    okn = true;
+                }
+                else
+                    okn = cell_con2prim(o, c, f.g, stored.p, pn);
+            }
             if (!okn)
             {
                 record_error(st, cfl && !prep ? 4 : 2,
