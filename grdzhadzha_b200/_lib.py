@@ -117,6 +117,13 @@ class Error(C.Structure):
 _P = C.POINTER
 _dp = _P(C.c_double)
 _vp = C.c_void_p
+class KitpConfig(C.Structure):
+    """grhd_kitp_config: the binary-PN disk driver's source-term settings."""
+    _fields_ = [(n, C.c_double) for n in (
+        "alpha_viscosity", "viscosity_beta", "rho_floor", "sink_size",
+        "sink_rate", "sink_shape")]
+
+
 class AdjointTorus(C.Structure):
     """grhd_adjoint_torus: the eight differentiable parameters (amplitude,
     entropy, spin, mode_amplitude[5]) and the fixed ones."""
@@ -192,6 +199,16 @@ SIGNATURES = {
     "grhd_ensemble_set_barrier_test": (C.c_int, [_vp, C.c_uint,
                                                  C.c_double]),
     "grhd_ensemble_launch_count": (C.c_longlong, [_vp]),
+    "grhd_default_kitp_config": (None, [_P(KitpConfig)]),
+    "grhd_kitp_viscous_rhs": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_int64,
+                                        _P(Box), _P(KitpConfig), C.c_double,
+                                        _vp]),
+    "grhd_kitp_sink_rhs": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_int64,
+                                     _P(Box), _P(KitpConfig), C.c_double,
+                                     _vp]),
+    "grhd_kitp_sink_decay": (C.c_int, [_vp, _vp, C.c_int64, _P(Box),
+                                       _P(KitpConfig), C.c_double, C.c_double,
+                                       _vp]),
     "grhd_default_adjoint_torus": (None, [_P(AdjointTorus)]),
     "grhd_adjoint_unit_entropy": (C.c_int, [_P(Params), _P(AdjointTorus),
                                             _dp]),

@@ -6,6 +6,7 @@
 #include "grhd_b200.h"
 #include "grhd_initial_data.cuh"
 #include "grhd_kernels.cuh"
+#include "grhd_kitp.cuh"
 
 #include <cmath>
 #include <cstdio>
@@ -1100,6 +1101,123 @@ int grhd_accretion(grhd_ctx *ctx, double *mdot_last, double *integral,
 long long grhd_launch_count(const grhd_ctx *ctx)
 {
     return ctx ? ctx->launches : 0;
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------
+// Source terms of the binary-PN disk driver (grhd_kitp.cuh).
+namespace {
+
+int kitp_setup(grhd_ctx *ctx, const void *state, const grhd_box *box,
+               int64_t state_cs, const grhd_kitp_config *cfg, double time,
+               BoxDev &b, KitpDev &k)
+{
+    int st = common_checks(ctx, state, box);
+    if (st)
+        return st;
+    if (!cfg)
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, nullptr,
+                         0.0, "null source-term configuration");
+    if (ctx->params.background != GRHD_BG_BINARY_PN)
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, nullptr,
+                         0.0, "the disk driver's source terms need the "
+                              "binary post-Newtonian background");
+    b = make_box(box, state_cs);
+    if (state_cs < b.gvol())
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, nullptr,
+                         0.0, "state stride smaller than the ghosted box");
+    k.alpha = cfg->alpha_viscosity;
+    k.beta = cfg->viscosity_beta;
+    k.rho_floor_cfg = cfg->rho_floor;
+    k.sink_size = cfg->sink_size;
+    k.sink_rate = cfg->sink_rate;
+    k.sink_shape = cfg->sink_shape;
+    k.mass[0] = ctx->params.pn_mass_1;
+    k.mass[1] = ctx->params.pn_mass_2;
+    double v1[3], v2[3];
+    pn_state(ctx->params, time, k.body[0], k.body[1], v1, v2);
+    k.atmo_rho_floor = ctx->params.rho_floor;
+    return GRHD_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+void grhd_default_kitp_config(grhd_kitp_config *c)
+{
+    if (!c)
+        return;
+    // SimulationConfig defaults, Main_GRHDLevelDataBinaryPNKITPDisk.cpp:63-71
+    c->alpha_viscosity = 0.03;
+    c->viscosity_beta = 0.0;
+    c->rho_floor = 1.0e-10;
+    c->sink_size = 1.0;
+    c->sink_rate = 1.0e4;
+    c->sink_shape = 4.0;
+}
+
+int grhd_kitp_viscous_rhs(grhd_ctx *ctx, double *rhs, int64_t rhs_cs,
+                          const double *state, int64_t state_cs,
+                          const grhd_box *box, const grhd_kitp_config *cfg,
+                          double time, void *stream)
+{
+    BoxDev b;
+    KitpDev k;
+    int st = kitp_setup(ctx, state, box, state_cs, cfg, time, b, k);
+    if (st)
+        return st;
+    if (!rhs || rhs_cs < b.ivol())
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, nullptr,
+                         0.0, "null rhs or rhs stride too small");
+    if (cfg->alpha_viscosity == 0.0)
+        return GRHD_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    ++ctx->launches;
+    launch_kitp_viscous_rhs(rhs, rhs_cs, state, b, ctx->opt, k, s);
+    GRHD_CUDA(ctx, cudaGetLastError());
+    return GRHD_OK;
+}
+
+int grhd_kitp_sink_rhs(grhd_ctx *ctx, double *rhs, int64_t rhs_cs,
+                       const double *state, int64_t state_cs,
+                       const grhd_box *box, const grhd_kitp_config *cfg,
+                       double time, void *stream)
+{
+    BoxDev b;
+    KitpDev k;
+    int st = kitp_setup(ctx, state, box, state_cs, cfg, time, b, k);
+    if (st)
+        return st;
+    if (!rhs || rhs_cs < b.ivol())
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, nullptr,
+                         0.0, "null rhs or rhs stride too small");
+    if (cfg->sink_rate == 0.0 || cfg->sink_size <= 0.0)
+        return GRHD_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    ++ctx->launches;
+    launch_kitp_sink_rhs(rhs, rhs_cs, state, b, ctx->opt, k, s);
+    GRHD_CUDA(ctx, cudaGetLastError());
+    return GRHD_OK;
+}
+
+int grhd_kitp_sink_decay(grhd_ctx *ctx, double *state, int64_t state_cs,
+                         const grhd_box *box, const grhd_kitp_config *cfg,
+                         double time, double dt, void *stream)
+{
+    BoxDev b;
+    KitpDev k;
+    int st = kitp_setup(ctx, state, box, state_cs, cfg, time, b, k);
+    if (st)
+        return st;
+    if (cfg->sink_rate == 0.0 || cfg->sink_size <= 0.0)
+        return GRHD_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    ++ctx->launches;
+    launch_kitp_sink_decay(state, b, ctx->opt, k, dt, s);
+    GRHD_CUDA(ctx, cudaGetLastError());
+    return GRHD_OK;
 }
 
 } // extern "C"

@@ -1,0 +1,36 @@
+// grhd_kitp.cuh -- source terms of the reference's binary-PN disk production
+// driver (Examples/GRHDLevelDataBinaryPNKITPDisk/
+// Main_GRHDLevelDataBinaryPNKITPDisk.cpp): the alpha-viscosity stress
+// divergence (:676-806) and the two point-mass sinks (:557-662), on the
+// device, FP64.
+#pragma once
+
+#include "grhd_kernels.cuh"
+
+namespace grhd {
+
+// The driver's SimulationConfig fields these terms read (:63, :67-71), the
+// binary's masses and body positions at the evaluation time, and the
+// atmosphere floor that switches them off.
+struct KitpDev
+{
+    double alpha, beta, rho_floor_cfg, sink_size, sink_rate, sink_shape;
+    double mass[2];
+    double body[2][3];
+    double atmo_rho_floor;
+};
+
+// rhs (interior, 5 components, stride rcs) -= d/dx F_x + d/dy F_y of the
+// viscous stress flux (add_kitp_viscous_rhs, :772-806).
+void launch_kitp_viscous_rhs(double *rhs, int64_t rcs, const double *state,
+                             const BoxDev &b, const Options &o,
+                             const KitpDev &k, cudaStream_t s);
+// rhs -= rate * conserved (add_kitp_sink_rhs, :567-610).
+void launch_kitp_sink_rhs(double *rhs, int64_t rcs, const double *state,
+                          const BoxDev &b, const Options &o, const KitpDev &k,
+                          cudaStream_t s);
+// conserved *= exp(-rate dt) (apply_kitp_sink_decay, :612-662).
+void launch_kitp_sink_decay(double *state, const BoxDev &b, const Options &o,
+                            const KitpDev &k, double dt, cudaStream_t s);
+
+} // namespace grhd

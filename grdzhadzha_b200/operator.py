@@ -155,6 +155,18 @@ class LevelBox:
                            device=self.state.device)
 
 
+def kitp_config(**kw) -> L.KitpConfig:
+    """The disk driver's source-term settings (SimulationConfig,
+    Main_GRHDLevelDataBinaryPNKITPDisk.cpp:63-71 defaults) with
+    overrides."""
+    lib = L.load()
+    c = L.KitpConfig()
+    lib.grhd_default_kitp_config(C.byref(c))
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
 def _ptr(t: torch.Tensor):
     if not t.is_cuda or t.dtype != torch.float64 or not t.is_contiguous():
         raise ValueError("expected a contiguous CUDA float64 tensor")
@@ -328,6 +340,36 @@ class _OperatorBase:
         self._check(self._lib.grhd_perturb_density(
             self._ctx, _ptr(state.state), state.comp_stride(), C.byref(b),
             amplitude, seed, time, _stream()))
+
+    # ---- the binary-PN disk driver's source terms ----
+
+    def kitp_viscous_rhs(self, rhs: torch.Tensor, state: LevelBox,
+                         config=None, time=0.0):
+        """add_kitp_viscous_rhs (Examples/GRHDLevelDataBinaryPNKITPDisk/
+        Main_GRHDLevelDataBinaryPNKITPDisk.cpp:772-806): rhs -= the
+        alpha-viscosity stress divergence in x and y."""
+        cfg = config if config is not None else kitp_config()
+        b = state.c_box()
+        self._check(self._lib.grhd_kitp_viscous_rhs(
+            self._ctx, _ptr(rhs), rhs[0].numel(), _ptr(state.state),
+            state.comp_stride(), C.byref(b), C.byref(cfg), time, _stream()))
+
+    def kitp_sink_rhs(self, rhs: torch.Tensor, state: LevelBox, config=None,
+                      time=0.0):
+        """add_kitp_sink_rhs (:567-610)."""
+        cfg = config if config is not None else kitp_config()
+        b = state.c_box()
+        self._check(self._lib.grhd_kitp_sink_rhs(
+            self._ctx, _ptr(rhs), rhs[0].numel(), _ptr(state.state),
+            state.comp_stride(), C.byref(b), C.byref(cfg), time, _stream()))
+
+    def kitp_sink_decay(self, state: LevelBox, time, dt, config=None):
+        """apply_kitp_sink_decay (:612-662) with the bodies at `time`."""
+        cfg = config if config is not None else kitp_config()
+        b = state.c_box()
+        self._check(self._lib.grhd_kitp_sink_decay(
+            self._ctx, _ptr(state.state), state.comp_stride(), C.byref(b),
+            C.byref(cfg), time, dt, _stream()))
 
     # ---- instrumentation ----
 

@@ -356,6 +356,41 @@ int grhd_profile_read(grhd_ctx *ctx, double ms[GRHD_K_NUM_CLASSES],
 /* Total number of kernels this context has launched. */
 long long grhd_launch_count(const grhd_ctx *ctx);
 
+/* ---- binary-PN disk driver source terms ----
+ * The source terms the reference's production driver adds to the operator
+ * (Examples/GRHDLevelDataBinaryPNKITPDisk/
+ * Main_GRHDLevelDataBinaryPNKITPDisk.cpp): its SimulationConfig fields
+ * (:63, :67-71).  They need the binary-PN operator (body masses and orbit
+ * from its params at the given operator time). */
+typedef struct grhd_kitp_config
+{
+    double alpha_viscosity, viscosity_beta, rho_floor, sink_size, sink_rate,
+        sink_shape;
+} grhd_kitp_config;
+
+void grhd_default_kitp_config(grhd_kitp_config *config);
+/* add_kitp_viscous_rhs (:772-806): rhs (interior, 5 components) -= the
+ * central difference in x and y of the alpha-viscosity stress flux
+ * (viscous_flux_for_cell, :700-770) built from the state's stored
+ * primitives; neighbours clamped to the problem domain (:664-674). */
+int grhd_kitp_viscous_rhs(grhd_ctx *ctx, double *rhs, int64_t rhs_comp_stride,
+                          const double *state, int64_t state_comp_stride,
+                          const grhd_box *box, const grhd_kitp_config *config,
+                          double time, void *stream);
+/* add_kitp_sink_rhs (:567-610): rhs -= rate * conserved where the stored
+ * density is above 10 x the atmosphere floor. */
+int grhd_kitp_sink_rhs(grhd_ctx *ctx, double *rhs, int64_t rhs_comp_stride,
+                       const double *state, int64_t state_comp_stride,
+                       const grhd_box *box, const grhd_kitp_config *config,
+                       double time, void *stream);
+/* apply_kitp_sink_decay (:612-662): conserved *= exp(-rate dt) with the
+ * bodies at operator time `time` (the driver passes the step's mid time,
+ * :874). */
+int grhd_kitp_sink_decay(grhd_ctx *ctx, double *state,
+                         int64_t state_comp_stride, const grhd_box *box,
+                         const grhd_kitp_config *config, double time,
+                         double dt, void *stream);
+
 /* ---- batched ensemble (new; no reference counterpart) ----
  * Many independent single-box problems on Kerr-Schild backgrounds, of any
  * sizes, spins, EOS and floors, advanced together: every call runs `steps`

@@ -2506,3 +2506,213 @@ static void cons_fill_job(void *ctx, int k0, int k1, int slot)
                 store_cons(b, state, idx, &c);
             }
 }
+
+/* ------------------------------------------------------------------------ */
+/* KITP disk driver source terms,                                            */
+/* Examples/GRHDLevelDataBinaryPNKITPDisk/Main_GRHDLevelDataBinaryPNKITPDisk.cpp */
+/* ------------------------------------------------------------------------ */
+
+/* sink_kernel, :557-565 */
+static double kitp_sink_kernel(double r2, double sink_radius,
+                               const orc_kitp_config *k)
+{
+    if (sink_radius <= 0.0 || k->sink_rate == 0.0)
+        return 0.0;
+    const double size2 = sink_radius * sink_radius;
+    return exp(-pow(r2 / size2, 0.5 * k->sink_shape));
+}
+
+/* the summed sink rate of both bodies at a cell (:584-597, :633-650) */
+static double kitp_sink_rate(const orc_params *p, const orc_kitp_config *k,
+                             const double bp[2][3], int i, int j, int l)
+{
+    double x, y, z;
+    cell_position(p, i, j, l, &x, &y, &z);
+    const double pos[3] = {x, y, z};
+    const double mass[2] = {p->pn_mass_1, p->pn_mass_2};
+    double rate = 0.0;
+    for (int b = 0; b < 2; ++b)
+    {
+        double r2 = 0.0;
+        for (int d = 0; d < 3; ++d)
+        {
+            const double dd = pos[d] - bp[b][d];
+            r2 += dd * dd;
+        }
+        rate += k->sink_rate * kitp_sink_kernel(r2, k->sink_size * mass[b], k);
+    }
+    return rate;
+}
+
+static void kitp_bodies(const orc_params *p, double t, double bp[2][3])
+{
+    double v1[3], v2[3];
+    pn_state(p, t, bp[0], bp[1], v1, v2);
+}
+
+/* add_kitp_sink_rhs, :567-610 */
+void orc_kitp_sink_rhs(const orc_params *p, const orc_kitp_config *k,
+                       const orc_box *b, const double *state, double *rhs,
+                       int64_t rcs, double t)
+{
+    if (k->sink_rate == 0.0 || k->sink_size <= 0.0)
+        return;
+    double bp[2][3];
+    kitp_bodies(p, t, bp);
+    const int nx = b->hi[0] - b->lo[0] + 1, ny = b->hi[1] - b->lo[1] + 1;
+    for (int l = b->lo[2]; l <= b->hi[2]; ++l)
+        for (int j = b->lo[1]; j <= b->hi[1]; ++j)
+            for (int i = b->lo[0]; i <= b->hi[0]; ++i)
+            {
+                const int64_t g = fab_index(b, i, j, l);
+                const Prim pr = load_prim(b, state, g);
+                if (pr.rho <= 10.0 * p->atmo_rho_floor)
+                    continue;
+                const double rate = kitp_sink_rate(p, k, bp, i, j, l);
+                if (rate == 0.0)
+                    continue;
+                const Cons c = load_cons(b, state, g);
+                const int64_t r = (i - b->lo[0]) +
+                                  (int64_t)nx * ((j - b->lo[1]) +
+                                                 (int64_t)ny * (l - b->lo[2]));
+                rhs[0 * rcs + r] -= rate * c.D;
+                rhs[4 * rcs + r] -= rate * c.tau;
+                for (int d = 0; d < 3; ++d)
+                    rhs[(1 + d) * rcs + r] -= rate * c.S[d];
+            }
+}
+
+/* apply_kitp_sink_decay, :612-662 (one box) */
+void orc_kitp_sink_decay(const orc_params *p, const orc_kitp_config *k,
+                         const orc_box *b, double *state, double t, double dt)
+{
+    if (k->sink_rate == 0.0 || k->sink_size <= 0.0)
+        return;
+    double bp[2][3];
+    kitp_bodies(p, t, bp);
+    const int64_t cs = b->comp_stride;
+    for (int l = b->lo[2]; l <= b->hi[2]; ++l)
+        for (int j = b->lo[1]; j <= b->hi[1]; ++j)
+            for (int i = b->lo[0]; i <= b->hi[0]; ++i)
+            {
+                const int64_t g = fab_index(b, i, j, l);
+                if (state[ORC_D * cs + g] <= 0.0)
+                    continue;
+                const double rate = kitp_sink_rate(p, k, bp, i, j, l);
+                if (rate == 0.0)
+                    continue;
+                const double decay = exp(-rate * dt);
+                state[ORC_D * cs + g] *= decay;
+                state[ORC_TAU * cs + g] *= decay;
+                state[ORC_S1 * cs + g] *= decay;
+                state[ORC_S2 * cs + g] *= decay;
+                state[ORC_S3 * cs + g] *= decay;
+            }
+}
+
+/* clamped_neighbor, :664-674 (clamped to the problem domain) */
+static int kitp_clamp(int v, int lo, int hi)
+{
+    return v < lo ? lo : (v > hi ? hi : v);
+}
+
+/* alpha_dynamic_viscosity, :676-698 */
+static double kitp_mu(const orc_params *p, const orc_kitp_config *k,
+                      const Prim *pr, const double pos[3],
+                      const double bp[2][3])
+{
+    if (k->alpha_viscosity == 0.0)
+        return 0.0;
+    const double mass[2] = {p->pn_mass_1, p->pn_mass_2};
+    double omega2 = 0.0;
+    for (int b = 0; b < 2; ++b)
+    {
+        double r2 = 1.0e-10;
+        for (int d = 0; d < 3; ++d)
+        {
+            const double dd = pos[d] - bp[b][d];
+            r2 += dd * dd;
+        }
+        omega2 += mass[b] * pow(r2, -1.5);
+    }
+    const double cs2 = p->gamma * pr->p / dmax(pr->rho, k->rho_floor);
+    return pr->rho * k->alpha_viscosity * cs2 / sqrt(dmax(omega2, 1.0e-300));
+}
+
+/* viscous_flux_for_cell, :700-770; flux[0..2] = S_x, S_y, tau */
+static void kitp_viscous_flux(const orc_params *p, const orc_kitp_config *k,
+                              const orc_box *b, const double *state, int i,
+                              int j, int l, int dir, const double bp[2][3],
+                              double flux[3])
+{
+    flux[0] = flux[1] = flux[2] = 0.0;
+    const Prim pr = load_prim(b, state, fab_index(b, i, j, l));
+    if (pr.rho <= 10.0 * p->atmo_rho_floor)
+        return;
+    double x, y, z;
+    cell_position(p, i, j, l, &x, &y, &z);
+    const double pos[3] = {x, y, z};
+    const double mu = kitp_mu(p, k, &pr, pos, bp);
+    if (mu == 0.0)
+        return;
+    double gradv[2][2];
+    const int iv[3] = {i, j, l};
+    for (int c = 0; c < 2; ++c)
+    {
+        int m[3] = {i, j, l}, q[3] = {i, j, l};
+        m[c] = kitp_clamp(iv[c] - 1, b->dlo[c], b->dhi[c]);
+        q[c] = kitp_clamp(iv[c] + 1, b->dlo[c], b->dhi[c]);
+        const int span = q[c] - m[c];
+        const double den = (span > 1 ? span : 1) * p->dx;
+        const Prim pm = load_prim(b, state, fab_index(b, m[0], m[1], m[2]));
+        const Prim pq = load_prim(b, state, fab_index(b, q[0], q[1], q[2]));
+        for (int v = 0; v < 2; ++v)
+            gradv[v][c] = (pq.v[v] - pm.v[v]) / den;
+    }
+    const double divergence = gradv[0][0] + gradv[1][1];
+    double tau[2][2];
+    for (int a = 0; a < 2; ++a)
+        for (int c = 0; c < 2; ++c)
+            tau[a][c] = mu * (gradv[a][c] + gradv[c][a] +
+                              (k->viscosity_beta - 2.0 / 3.0) *
+                                  (double)(a == c) * divergence);
+    flux[0] = -tau[dir][0];
+    flux[1] = -tau[dir][1];
+    flux[2] = -tau[dir][0] * pr.v[0] - tau[dir][1] * pr.v[1];
+}
+
+/* add_kitp_viscous_rhs, :772-806 */
+void orc_kitp_viscous_rhs(const orc_params *p, const orc_kitp_config *k,
+                          const orc_box *b, const double *state, double *rhs,
+                          int64_t rcs, double t)
+{
+    if (k->alpha_viscosity == 0.0)
+        return;
+    double bp[2][3];
+    kitp_bodies(p, t, bp);
+    const int nx = b->hi[0] - b->lo[0] + 1, ny = b->hi[1] - b->lo[1] + 1;
+    for (int l = b->lo[2]; l <= b->hi[2]; ++l)
+        for (int j = b->lo[1]; j <= b->hi[1]; ++j)
+            for (int i = b->lo[0]; i <= b->hi[0]; ++i)
+            {
+                const int64_t r = (i - b->lo[0]) +
+                                  (int64_t)nx * ((j - b->lo[1]) +
+                                                 (int64_t)ny * (l - b->lo[2]));
+                const int iv[3] = {i, j, l};
+                for (int d = 0; d < 2; ++d)
+                {
+                    int lo[3] = {i, j, l}, hi[3] = {i, j, l};
+                    lo[d] = kitp_clamp(iv[d] - 1, b->dlo[d], b->dhi[d]);
+                    hi[d] = kitp_clamp(iv[d] + 1, b->dlo[d], b->dhi[d]);
+                    double fl[3], fh[3];
+                    kitp_viscous_flux(p, k, b, state, lo[0], lo[1], lo[2], d,
+                                      bp, fl);
+                    kitp_viscous_flux(p, k, b, state, hi[0], hi[1], hi[2], d,
+                                      bp, fh);
+                    rhs[4 * rcs + r] -= (fh[2] - fl[2]) / (2.0 * p->dx);
+                    rhs[1 * rcs + r] -= (fh[0] - fl[0]) / (2.0 * p->dx);
+                    rhs[2 * rcs + r] -= (fh[1] - fl[1]) / (2.0 * p->dx);
+                }
+            }
+}
+

@@ -241,6 +241,31 @@ void orc_disk_diagnostics(const orc_params *p, const orc_box *box,
                           const int lo[3], const int hi[3],
                           const double *state, double time, double *out7);
 
+
+/* ---- KITP disk driver source terms (the binary-PN production driver) ----
+ * Examples/GRHDLevelDataBinaryPNKITPDisk/Main_GRHDLevelDataBinaryPNKITPDisk.cpp
+ * SimulationConfig fields (:67-71) and rho_floor (:63) used by them. */
+typedef struct orc_kitp_config
+{
+    double alpha_viscosity, viscosity_beta, rho_floor, sink_size, sink_rate,
+        sink_shape;
+} orc_kitp_config;
+/* add_kitp_viscous_rhs (:772-806): rhs (interior, 5 comps) -= the central
+ * difference of the alpha-viscosity stress flux in x and y, from the
+ * state's stored primitives, binary at operator time t. */
+void orc_kitp_viscous_rhs(const orc_params *p, const orc_kitp_config *k,
+                          const orc_box *box, const double *state,
+                          double *rhs, int64_t rhs_comp_stride, double t);
+/* add_kitp_sink_rhs (:567-610): rhs -= rate * conserved. */
+void orc_kitp_sink_rhs(const orc_params *p, const orc_kitp_config *k,
+                       const orc_box *box, const double *state, double *rhs,
+                       int64_t rhs_comp_stride, double t);
+/* apply_kitp_sink_decay (:612-662): conserved *= exp(-rate dt) at binary
+ * time t (the driver passes the step's mid time). */
+void orc_kitp_sink_decay(const orc_params *p, const orc_kitp_config *k,
+                         const orc_box *box, double *state, double t,
+                         double dt);
+
 #ifdef __cplusplus
 }
 #endif

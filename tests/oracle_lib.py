@@ -99,6 +99,39 @@ class MichelConfig(C.Structure):
 _lib = None
 
 
+class KitpConfig(C.Structure):
+    """orc_kitp_config: the binary-PN disk driver's source-term settings
+    (Main_GRHDLevelDataBinaryPNKITPDisk.cpp SimulationConfig :63, :67-71)."""
+    _fields_ = [(n, C.c_double) for n in (
+        "alpha_viscosity", "viscosity_beta", "rho_floor", "sink_size",
+        "sink_rate", "sink_shape")]
+
+
+def kitp_config(**kw) -> KitpConfig:
+    """The driver's defaults (:63, :67-71), overridden by kw."""
+    k = KitpConfig(0.03, 0.0, 1.0e-10, 1.0, 1.0e4, 4.0)
+    for name, v in kw.items():
+        setattr(k, name, v)
+    return k
+
+
+def kitp_viscous_rhs(p, k, box, state, rhs, time=0.0):
+    """rhs (flat, 5 x interior) -= the viscous stress divergence."""
+    lib().orc_kitp_viscous_rhs(C.byref(p), C.byref(k), C.byref(box),
+                               _dp(state), _dp(rhs), interior_cells(box),
+                               time)
+
+
+def kitp_sink_rhs(p, k, box, state, rhs, time=0.0):
+    lib().orc_kitp_sink_rhs(C.byref(p), C.byref(k), C.byref(box), _dp(state),
+                            _dp(rhs), interior_cells(box), time)
+
+
+def kitp_sink_decay(p, k, box, state, time, dt):
+    lib().orc_kitp_sink_decay(C.byref(p), C.byref(k), C.byref(box),
+                              _dp(state), time, dt)
+
+
 def build():
     subprocess.run(["make", "-s", "-C", _ORACLE_DIR], check=True)
 
@@ -162,6 +195,11 @@ def lib():
                                                          C.c_double]
         L.orc_disk_diagnostics.argtypes = [P, B, C.c_int * 3, C.c_int * 3, dp,
                                            C.c_double, dp]
+        K = C.POINTER(KitpConfig)
+        L.orc_kitp_viscous_rhs.argtypes = [P, K, B, dp, dp, i64, C.c_double]
+        L.orc_kitp_sink_rhs.argtypes = [P, K, B, dp, dp, i64, C.c_double]
+        L.orc_kitp_sink_decay.argtypes = [P, K, B, dp, C.c_double,
+                                          C.c_double]
         _lib = L
     return _lib
 
