@@ -117,6 +117,18 @@ class Error(C.Structure):
 _P = C.POINTER
 _dp = _P(C.c_double)
 _vp = C.c_void_p
+class CheckpointHeader(C.Structure):
+    """grhd_checkpoint_header (the KITPCHK1 header fields)."""
+    _fields_ = [("num_components", C.c_int), ("num_cells", C.c_int),
+                ("num_z_cells", C.c_int), ("num_ghosts", C.c_int),
+                ("steps", C.c_int), ("frame_index", C.c_int),
+                ("time", C.c_double), ("next_output_time", C.c_double),
+                ("next_checkpoint_time", C.c_double),
+                ("recovery_totals", C.c_longlong * 4),
+                ("diagnostics", C.c_double * 7),
+                ("diagnostic_counts", C.c_longlong * 3)]
+
+
 class KitpConfig(C.Structure):
     """grhd_kitp_config: the binary-PN disk driver's source-term settings."""
     _fields_ = [(n, C.c_double) for n in (
@@ -199,6 +211,14 @@ SIGNATURES = {
     "grhd_ensemble_set_barrier_test": (C.c_int, [_vp, C.c_uint,
                                                  C.c_double]),
     "grhd_ensemble_launch_count": (C.c_longlong, [_vp]),
+    "grhd_disk_diagnostics": (C.c_int, [_vp, _vp, C.c_int64, _P(Box),
+                                        C.c_double, _dp, _vp]),
+    "grhd_checkpoint_write": (C.c_int, [C.c_char_p, _P(CheckpointHeader),
+                                        C.c_char_p, _vp, C.c_int64, _P(Box),
+                                        C.c_char_p, C.c_int, _vp]),
+    "grhd_checkpoint_read": (C.c_int, [C.c_char_p, _P(CheckpointHeader),
+                                       C.c_char_p, _vp, C.c_int64, _P(Box),
+                                       C.c_char_p, C.c_int, _vp]),
     "grhd_default_kitp_config": (None, [_P(KitpConfig)]),
     "grhd_kitp_viscous_rhs": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_int64,
                                         _P(Box), _P(KitpConfig), C.c_double,

@@ -9,7 +9,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _ROOT = os.path.dirname(_HERE)
 CSRC = os.path.join(_HERE, "csrc")
 SOURCES = ["grhd_kernels.cu", "grhd_initial_data.cu", "grhd_capi.cu",
-           "grhd_ensemble.cu", "grhd_adjoint.cu", "grhd_kitp.cu"]
+           "grhd_ensemble.cu", "grhd_adjoint.cu", "grhd_kitp.cu",
+           "grhd_io.cu"]
 OUTPUT = os.path.join(_HERE, "libgrhd_b200.so")
 
 NVCC_FLAGS = [

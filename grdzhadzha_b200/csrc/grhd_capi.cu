@@ -6,11 +6,14 @@
 #include "grhd_b200.h"
 #include "grhd_initial_data.cuh"
 #include "grhd_kernels.cuh"
+#include "grhd_io.cuh"
 #include "grhd_kitp.cuh"
 
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <string>
 #include <mutex>
 #include <new>
 #include <vector>
@@ -1217,6 +1220,282 @@ int grhd_kitp_sink_decay(grhd_ctx *ctx, double *state, int64_t state_cs,
     ++ctx->launches;
     launch_kitp_sink_decay(state, b, ctx->opt, k, dt, s);
     GRHD_CUDA(ctx, cudaGetLastError());
+    return GRHD_OK;
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------
+// Diagnostics and checkpoints of the example drivers (grhd_io.cuh).
+namespace {
+
+int io_error(char *err, int cap, const char *msg, int status)
+{
+    if (err && cap > 0)
+        std::snprintf(err, (size_t)cap, "%s", msg);
+    return status;
+}
+
+template <typename V> void put(std::FILE *f, const V &v, bool &ok)
+{
+    ok = ok && std::fwrite(&v, sizeof(V), 1, f) == 1;
+}
+
+template <typename V> bool get(std::FILE *f, V &v)
+{
+    return std::fread(&v, sizeof(V), 1, f) == 1;
+}
+
+// The header fields of read_checkpoint_header
+// (Main_GRHDLevelDataBinaryPNKITPDisk.cpp:1289-1345) up to the state.
+int read_header(std::FILE *f, grhd_checkpoint_header &h, std::string &sig,
+                uint64_t &count, char *err, int cap)
+{
+    char magic[8];
+    if (std::fread(magic, 1, 8, f) != 8 || std::memcmp(magic, "KITPCHK1", 8))
+        return io_error(err, cap, "not a KITP checkpoint",
+                        GRHD_ERR_INVALID_ARG);
+    uint32_t version;
+    int32_t nc, ncell, nz, ng, steps, frame;
+    if (!get(f, version) || !get(f, nc) || !get(f, ncell) || !get(f, nz) ||
+        !get(f, ng))
+        return io_error(err, cap, "checkpoint ended unexpectedly",
+                        GRHD_ERR_INVALID_ARG);
+    if (version != 1 || nc < kStateComps)
+        return io_error(err, cap, "unsupported KITP checkpoint format",
+                        GRHD_ERR_INVALID_ARG);
+    h.num_components = nc;
+    h.num_cells = ncell;
+    h.num_z_cells = nz;
+    h.num_ghosts = ng;
+    bool ok = get(f, steps) && get(f, frame) && get(f, h.time) &&
+              get(f, h.next_output_time) && get(f, h.next_checkpoint_time);
+    h.steps = steps;
+    h.frame_index = frame;
+    for (int q = 0; q < 4 && ok; ++q)
+    {
+        uint64_t v;
+        ok = get(f, v);
+        h.recovery_totals[q] = (long long)v;
+    }
+    for (int q = 0; q < 7 && ok; ++q)
+        ok = get(f, h.diagnostics[q]);
+    for (int q = 0; q < 3 && ok; ++q)
+    {
+        uint64_t v;
+        ok = get(f, v);
+        h.diagnostic_counts[q] = (long long)v;
+    }
+    uint64_t ssize = 0;
+    ok = ok && get(f, ssize);
+    if (!ok)
+        return io_error(err, cap, "checkpoint ended unexpectedly",
+                        GRHD_ERR_INVALID_ARG);
+    if (ssize > 16384)
+        return io_error(err, cap,
+                        "invalid checkpoint configuration signature",
+                        GRHD_ERR_INVALID_ARG);
+    sig.assign((size_t)ssize, '\0');
+    if ((ssize && std::fread(&sig[0], 1, (size_t)ssize, f) != ssize) ||
+        !get(f, count))
+        return io_error(err, cap, "checkpoint ended unexpectedly",
+                        GRHD_ERR_INVALID_ARG);
+    return GRHD_OK;
+}
+
+// The box must be the checkpoint's storage box: the domain (num_cells^2 x
+// num_z_cells) grown by num_ghosts (checkpoint_storage_box, :1358-1363).
+bool storage_matches(const grhd_box *box, int ncell, int nz, int ng)
+{
+    if (!valid_box(box) || !box_is_domain(box) || box->ghost != ng)
+        return false;
+    const int n[3] = {ncell, ncell, nz};
+    for (int d = 0; d < 3; ++d)
+        if (box->hi[d] - box->lo[d] + 1 != n[d])
+            return false;
+    return true;
+}
+
+} // namespace
+
+extern "C" {
+
+int grhd_disk_diagnostics(grhd_ctx *ctx, const double *state,
+                          int64_t state_cs, const grhd_box *box, double time,
+                          double out[7], void *stream)
+{
+    int st = common_checks(ctx, state, box);
+    if (st)
+        return st;
+    if (!out)
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, nullptr,
+                         0.0, "null output");
+    const BoxDev b = make_box(box, state_cs);
+    if (state_cs < b.gvol())
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, nullptr,
+                         0.0, "state stride smaller than the ghosted box");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nb = diagnostics_blocks(b);
+    double *part = nullptr;
+    GRHD_CUDA(ctx, cudaMallocAsync((void **)&part, sizeof(double) * 7 * nb, s));
+    ++ctx->launches;
+    launch_diagnostics(state, b, make_background(ctx->params, time),
+                       ctx->opt, part, s);
+    std::vector<double> h((size_t)7 * nb);
+    cudaError_t e = cudaMemcpyAsync(h.data(), part, sizeof(double) * 7 * nb,
+                                    cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaFreeAsync(part, s);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess)
+        return cuda_error(ctx, e, "grhd_disk_diagnostics");
+    double r[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1.0};
+    for (int q = 0; q < nb; ++q)
+    {
+        for (int c = 0; c < 3; ++c)
+            r[c] += h[(size_t)q * 7 + c];
+        for (int c = 3; c < 7; ++c)
+            r[c] = std::fmax(r[c], h[(size_t)q * 7 + c]);
+    }
+    for (int c = 0; c < 7; ++c)
+        out[c] = r[c];
+    return GRHD_OK;
+}
+
+int grhd_checkpoint_write(const char *path, const grhd_checkpoint_header *h,
+                          const char *signature, const double *state,
+                          int64_t state_cs, const grhd_box *box, char *err,
+                          int err_cap, void *stream)
+{
+    if (!path || !h || !signature || !state)
+        return io_error(err, err_cap, "null argument", GRHD_ERR_INVALID_ARG);
+    if (h->num_components < kStateComps)
+        return io_error(err, err_cap, "fewer components than the GRHD state",
+                        GRHD_ERR_INVALID_ARG);
+    if (!storage_matches(box, h->num_cells, h->num_z_cells, h->num_ghosts))
+        return io_error(err, err_cap,
+                        "box is not the checkpoint's domain and ghosts",
+                        GRHD_ERR_INVALID_ARG);
+    const BoxDev b = make_box(box, state_cs);
+    if (state_cs < b.gvol())
+        return io_error(err, err_cap, "state stride too small",
+                        GRHD_ERR_INVALID_ARG);
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint64_t count = (uint64_t)h->num_components * (uint64_t)b.gvol();
+    std::vector<double> host((size_t)count);
+    double *dev = nullptr;
+    cudaError_t e = cudaMalloc((void **)&dev, count * sizeof(double));
+    if (e == cudaSuccess)
+    {
+        launch_state_to_checkpoint(state, b, h->num_components, dev, s);
+        e = cudaMemcpyAsync(host.data(), dev, count * sizeof(double),
+                            cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(s);
+        cudaFree(dev);
+    }
+    if (e != cudaSuccess)
+        return io_error(err, err_cap, cudaGetErrorString(e), GRHD_ERR_CUDA);
+    // write_checkpoint, :1385-1505: a temporary file renamed into place
+    const std::string tmp = std::string(path) + ".tmp";
+    std::FILE *f = std::fopen(tmp.c_str(), "wb");
+    if (!f)
+        return io_error(err, err_cap, "could not create checkpoint",
+                        GRHD_ERR_SETUP);
+    bool ok = std::fwrite("KITPCHK1", 1, 8, f) == 8;
+    put(f, (uint32_t)1, ok);
+    put(f, (int32_t)h->num_components, ok);
+    put(f, (int32_t)h->num_cells, ok);
+    put(f, (int32_t)h->num_z_cells, ok);
+    put(f, (int32_t)h->num_ghosts, ok);
+    put(f, (int32_t)h->steps, ok);
+    put(f, (int32_t)h->frame_index, ok);
+    put(f, h->time, ok);
+    put(f, h->next_output_time, ok);
+    put(f, h->next_checkpoint_time, ok);
+    for (int q = 0; q < 4; ++q)
+        put(f, (uint64_t)h->recovery_totals[q], ok);
+    for (int q = 0; q < 7; ++q)
+        put(f, h->diagnostics[q], ok);
+    for (int q = 0; q < 3; ++q)
+        put(f, (uint64_t)h->diagnostic_counts[q], ok);
+    const uint64_t ssize = std::strlen(signature);
+    put(f, ssize, ok);
+    ok = ok && std::fwrite(signature, 1, (size_t)ssize, f) == ssize;
+    put(f, count, ok);
+    ok = ok && std::fwrite(host.data(), sizeof(double), (size_t)count, f) ==
+                   count;
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok)
+        return io_error(err, err_cap, "failed while writing checkpoint",
+                        GRHD_ERR_SETUP);
+    if (std::rename(tmp.c_str(), path) != 0)
+        return io_error(err, err_cap, "could not finalize checkpoint",
+                        GRHD_ERR_SETUP);
+    return GRHD_OK;
+}
+
+int grhd_checkpoint_read(const char *path, grhd_checkpoint_header *h,
+                         const char *expected_signature, double *state,
+                         int64_t state_cs, const grhd_box *box, char *err,
+                         int err_cap, void *stream)
+{
+    if (!path || !h)
+        return io_error(err, err_cap, "null argument", GRHD_ERR_INVALID_ARG);
+    std::FILE *f = std::fopen(path, "rb");
+    if (!f)
+        return io_error(err, err_cap, "could not open checkpoint",
+                        GRHD_ERR_INVALID_ARG);
+    std::string sig;
+    uint64_t count = 0;
+    int st = read_header(f, *h, sig, count, err, err_cap);
+    if (st == GRHD_OK && expected_signature && sig != expected_signature)
+        st = io_error(err, err_cap,
+                      "checkpoint configuration does not match this run",
+                      GRHD_ERR_INVALID_ARG);
+    if (st != GRHD_OK || !state)
+    {
+        std::fclose(f);
+        return st;
+    }
+    if (!storage_matches(box, h->num_cells, h->num_z_cells, h->num_ghosts))
+    {
+        std::fclose(f);
+        return io_error(err, err_cap, "checkpoint grid does not match this run",
+                        GRHD_ERR_INVALID_ARG);
+    }
+    const BoxDev b = make_box(box, state_cs);
+    if (state_cs < b.gvol() ||
+        count != (uint64_t)h->num_components * (uint64_t)b.gvol())
+    {
+        std::fclose(f);
+        return io_error(err, err_cap,
+                        "checkpoint state size does not match the grid",
+                        GRHD_ERR_INVALID_ARG);
+    }
+    std::vector<double> host((size_t)count);
+    const bool ok =
+        std::fread(host.data(), sizeof(double), (size_t)count, f) == count;
+    std::fclose(f);
+    if (!ok)
+        return io_error(err, err_cap, "checkpoint state data is incomplete",
+                        GRHD_ERR_INVALID_ARG);
+    cudaStream_t s = (cudaStream_t)stream;
+    double *dev = nullptr;
+    cudaError_t e = cudaMalloc((void **)&dev, count * sizeof(double));
+    if (e == cudaSuccess)
+    {
+        e = cudaMemcpyAsync(dev, host.data(), count * sizeof(double),
+                            cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess)
+            launch_checkpoint_to_state(dev, b, h->num_components, state, s);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(s);
+        cudaFree(dev);
+    }
+    if (e != cudaSuccess)
+        return io_error(err, err_cap, cudaGetErrorString(e), GRHD_ERR_CUDA);
     return GRHD_OK;
 }
 

@@ -341,6 +341,17 @@ class _OperatorBase:
             self._ctx, _ptr(state.state), state.comp_stride(), C.byref(b),
             amplitude, seed, time, _stream()))
 
+    def disk_diagnostics(self, state: LevelBox, time=0.0) -> list:
+        """compute_diagnostics of the example drivers
+        (Main_GRHDLevelDataKerrSchildDisk.cpp:223-290): [mass, disk_mass,
+        tau, max_rho, max_pressure, max_velocity, max_lorentz_factor]."""
+        out = (C.c_double * 7)()
+        b = state.c_box()
+        self._check(self._lib.grhd_disk_diagnostics(
+            self._ctx, _ptr(state.state), state.comp_stride(), C.byref(b),
+            time, out, _stream()))
+        return list(out)
+
     # ---- the binary-PN disk driver's source terms ----
 
     def kitp_viscous_rhs(self, rhs: torch.Tensor, state: LevelBox,

@@ -391,6 +391,51 @@ int grhd_kitp_sink_decay(grhd_ctx *ctx, double *state,
                          const grhd_kitp_config *config, double time,
                          double dt, void *stream);
 
+/* ---- example drivers' diagnostics and checkpoints ---- */
+
+/* compute_diagnostics of the example drivers
+ * (Examples/GRHDLevelDataKerrSchildDisk/Main_GRHDLevelDataKerrSchildDisk.cpp:
+ * 223-290): out = mass, disk_mass (cells denser than 10 x the atmosphere
+ * floor), tau (proper-volume sums of D and tau), max rho, max pressure,
+ * max |v|, max W over the box interior, from the stored primitives.
+ * Synchronous. */
+int grhd_disk_diagnostics(grhd_ctx *ctx, const double *state,
+                          int64_t state_comp_stride, const grhd_box *box,
+                          double time, double out[7], void *stream);
+
+/* The header of a KITPCHK1 checkpoint (write_checkpoint /
+ * read_checkpoint_header, Examples/GRHDLevelDataBinaryPNKITPDisk/
+ * Main_GRHDLevelDataBinaryPNKITPDisk.cpp:1289-1505).  num_components is
+ * the driver's NUM_VARS (its GRHD components are the last 11, after the
+ * CCZ4 slots, which the writer fills with zeros and the reader ignores). */
+typedef struct grhd_checkpoint_header
+{
+    int num_components, num_cells, num_z_cells, num_ghosts, steps,
+        frame_index;
+    double time, next_output_time, next_checkpoint_time;
+    long long recovery_totals[4]; /* cells, failed, floored, resets */
+    double diagnostics[7];        /* as grhd_disk_diagnostics */
+    long long diagnostic_counts[3];
+} grhd_checkpoint_header;
+
+/* Writes the device state (11 components over the ghosted box, which must
+ * be the checkpoint's domain num_cells^2 x num_z_cells grown by
+ * num_ghosts) as a KITPCHK1 file the reference driver restarts from;
+ * `signature` is the driver's config_signature (:1203-1223).  On error
+ * err (err_cap bytes, may be NULL) receives the reference's message. */
+int grhd_checkpoint_write(const char *path,
+                          const grhd_checkpoint_header *header,
+                          const char *signature, const double *state,
+                          int64_t state_comp_stride, const grhd_box *box,
+                          char *err, int err_cap, void *stream);
+/* Reads a KITPCHK1 file: the header, and (state non-NULL) the GRHD
+ * components into the device state; expected_signature (may be NULL)
+ * must equal the file's. */
+int grhd_checkpoint_read(const char *path, grhd_checkpoint_header *header,
+                         const char *expected_signature, double *state,
+                         int64_t state_comp_stride, const grhd_box *box,
+                         char *err, int err_cap, void *stream);
+
 /* ---- batched ensemble (new; no reference counterpart) ----
  * Many independent single-box problems on Kerr-Schild backgrounds, of any
  * sizes, spins, EOS and floors, advanced together: every call runs `steps`
