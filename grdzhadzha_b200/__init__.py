@@ -9,6 +9,7 @@ from .operator import (  # noqa: F401
     LevelBox,
     RecoveryOptions,
     TimeDependentFixedBGLevelDataFiniteVolumeOperator,
+    level_exchange,
 )
 from ._lib import GRHDError, InvalidArgument  # noqa: F401
 from .ensemble import Ensemble  # noqa: F401

@@ -213,6 +213,9 @@ SIGNATURES = {
     "grhd_ensemble_launch_count": (C.c_longlong, [_vp]),
     "grhd_disk_diagnostics": (C.c_int, [_vp, _vp, C.c_int64, _P(Box),
                                         C.c_double, _dp, _vp]),
+    "grhd_level_exchange": (C.c_int, [_P(Box), _P(C.c_void_p),
+                                      _P(C.c_int64), C.c_int, C.c_char_p,
+                                      C.c_int, _vp]),
     "grhd_checkpoint_write": (C.c_int, [C.c_char_p, _P(CheckpointHeader),
                                         C.c_char_p, _vp, C.c_int64, _P(Box),
                                         C.c_char_p, C.c_int, _vp]),

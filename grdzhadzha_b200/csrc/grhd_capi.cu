@@ -9,6 +9,7 @@
 #include "grhd_io.cuh"
 #include "grhd_kitp.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -1360,6 +1361,70 @@ int grhd_disk_diagnostics(grhd_ctx *ctx, const double *state,
     }
     for (int c = 0; c < 7; ++c)
         out[c] = r[c];
+    return GRHD_OK;
+}
+
+int grhd_level_exchange(const grhd_box *boxes, double *const *states,
+                        const int64_t *strides, int count, char *err,
+                        int err_cap, void *stream)
+{
+    if (count < 0 || (count > 0 && (!boxes || !states || !strides)))
+        return io_error(err, err_cap, "null level arrays",
+                        GRHD_ERR_INVALID_ARG);
+    std::vector<BoxDev> b((size_t)count);
+    for (int q = 0; q < count; ++q)
+    {
+        if (!valid_box(&boxes[q]) || !states[q])
+            return io_error(err, err_cap, "invalid box or state",
+                            GRHD_ERR_INVALID_ARG);
+        b[q] = make_box(&boxes[q], strides[q]);
+        if (strides[q] < b[q].gvol())
+            return io_error(err, err_cap, "state stride too small",
+                            GRHD_ERR_INVALID_ARG);
+        for (int d = 0; d < 3; ++d)
+            if (boxes[q].domain_lo[d] != boxes[0].domain_lo[d] ||
+                boxes[q].domain_hi[d] != boxes[0].domain_hi[d])
+                return io_error(err, err_cap,
+                                "the boxes of a level share one domain",
+                                GRHD_ERR_INVALID_ARG);
+    }
+    // a DisjointBoxLayout: interiors do not overlap
+    for (int p = 0; p < count; ++p)
+        for (int q = p + 1; q < count; ++q)
+        {
+            bool overlap = true;
+            for (int d = 0; d < 3; ++d)
+                overlap = overlap && b[p].lo[d] <= b[q].hi[d] &&
+                          b[q].lo[d] <= b[p].hi[d];
+            if (overlap)
+                return io_error(err, err_cap, "box interiors overlap",
+                                GRHD_ERR_INVALID_ARG);
+        }
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int a = 0; a < count; ++a)
+        for (int q = 0; q < count; ++q)
+        {
+            if (q == a)
+                continue;
+            // ghosted box of a, inside the domain, intersected with the
+            // interior of q (disjoint from a's interior)
+            int lo[3], hi[3];
+            bool any = true;
+            for (int d = 0; d < 3; ++d)
+            {
+                lo[d] = std::max(std::max(b[a].glo[d], b[a].dlo[d]),
+                                 b[q].lo[d]);
+                hi[d] = std::min(std::min(b[a].ghi[d], b[a].dhi[d]),
+                                 b[q].hi[d]);
+                any = any && lo[d] <= hi[d];
+            }
+            if (any)
+                launch_copy_region(states[a], b[a], states[q], b[q], lo, hi,
+                                   s);
+        }
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return io_error(err, err_cap, cudaGetErrorString(e), GRHD_ERR_CUDA);
     return GRHD_OK;
 }
 

@@ -118,6 +118,25 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+__global__ void __launch_bounds__(256)
+    k_copy_region(double *__restrict__ dst, BoxDev db,
+                  const double *__restrict__ src, BoxDev sb, int lo0, int lo1,
+                  int lo2, int n0, int n1, int n2)
+{
+    const int64_t n = (int64_t)n0 * n1 * n2;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int i = lo0 + (int)(t % n0);
+        const int64_t r = t / n0;
+        const int j = lo1 + (int)(r % n1);
+        const int k = lo2 + (int)(r / n1);
+        const int64_t gd = db.gidx(i, j, k), gs = sb.gidx(i, j, k);
+        for (int c = 0; c < kStateComps; ++c)
+            dst[c * db.cs + gd] = src[c * sb.cs + gs];
+    }
+}
+
 int grid_of(int64_t n)
 {
     int64_t g = (n + 255) / 256;
@@ -148,6 +167,16 @@ void launch_checkpoint_to_state(const double *in, const BoxDev &b, int ncomp,
                                 double *state, cudaStream_t s)
 {
     k_from_checkpoint<<<grid_of(b.gvol()), 256, 0, s>>>(in, b, ncomp, state);
+}
+
+void launch_copy_region(double *dst, const BoxDev &db, const double *src,
+                        const BoxDev &sb, const int lo[3], const int hi[3],
+                        cudaStream_t s)
+{
+    const int n0 = hi[0] - lo[0] + 1, n1 = hi[1] - lo[1] + 1,
+              n2 = hi[2] - lo[2] + 1;
+    k_copy_region<<<grid_of((int64_t)n0 * n1 * n2), 256, 0, s>>>(
+        dst, db, src, sb, lo[0], lo[1], lo[2], n0, n1, n2);
 }
 
 } // namespace grhd

@@ -32,4 +32,11 @@ void launch_state_to_checkpoint(const double *state, const BoxDev &b,
 void launch_checkpoint_to_state(const double *in, const BoxDev &b, int ncomp,
                                 double *state, cudaStream_t s);
 
+// LevelData::exchange between two boxes of a level: the 11 components of
+// the cells [lo, hi] (level index space) from `src` (box sb) to `dst`
+// (box db).
+void launch_copy_region(double *dst, const BoxDev &db, const double *src,
+                        const BoxDev &sb, const int lo[3], const int hi[3],
+                        cudaStream_t s);
+
 } // namespace grhd

@@ -237,7 +237,10 @@ __device__ __forceinline__ bool shell_cell(const BoxDev &b, int64_t t, int &i,
 // (fill_conserved_outflow_boundaries_from_fixed_background, :113-177),
 // then, for every shell cell, the ghosted-box con2prim of the RHS into the
 // primitive cache (recover_primitives_from_fixed_background, :33-58).  The
-// fill itself is FP64 in both paths.
+// fill itself is FP64 in both paths.  Shell cells inside the domain hold
+// the owning boxes' values (after grhd_level_exchange); an excised one of
+// them keeps its frozen primitives, as it does as an interior cell, so a
+// level's RHS does not depend on how it is cut into boxes.
 template <typename T, bool CG = false>
 __device__ __forceinline__ void ghost_item(double *__restrict__ state,
                                            T *__restrict__ prim,
@@ -291,6 +294,13 @@ __device__ __forceinline__ void ghost_item(double *__restrict__ state,
             store_prim(state, b.cs, idx, pr);
             c = p2c(pr, tLL);
             store_cons(state, b.cs, idx, c);
+        }
+        else if (excised(o, i, j, k))
+        {
+            // a ghost that another box of the level owns: frozen like the
+            // owner's interior cell
+            store_pv(prim, b.pcs, idx, load_prim<CG>(state, b.cs, idx));
+            return;
         }
         else
             c = load_cons<CG>(state, b.cs, idx);
@@ -596,6 +606,7 @@ faces_tile(const T *__restrict__ prim, const T *__restrict__ src,
     // own-column z window P(k-1..k+2) and the z face below k0
     PVT<T> w0, w1, w2, w3;
     ConsT<T> Flo = zero_cons<T>();
+    double macc = 0.0;
     tile_geometry(Gb, bg, o, i0, j0, k0, tid);
     __syncthreads();
     {
@@ -612,6 +623,10 @@ faces_tile(const T *__restrict__ prim, const T *__restrict__ src,
             geo_load(Gb, nG, (bb + 1) * kGW + (a + 1), gr);
             average_geo(gl, gr, gf);
             Flo = face_flux(o, w0, w1, w2, w3, gf, 2);
+            // a box counts the sphere faces whose upper cell it holds, in
+            // every direction, so the boxes of a level count each once
+            if (MDOT && k0 == b.lo[2])
+                macc += mdot_face(o, ci, cj, k0 - 1, 2, gf, Flo.D);
         }
         // shift so that w0..w3 = P(k0-1 .. k0+2) after the next load
         w0 = w1;
@@ -620,7 +635,6 @@ faces_tile(const T *__restrict__ prim, const T *__restrict__ src,
     }
 
     int cur = 0;
-    double macc = 0.0;
     for (int k = k0; k <= k1; ++k)
     {
         T *Gc = Gb + cur * kGeoFields * nG;

@@ -155,6 +155,25 @@ class LevelBox:
                            device=self.state.device)
 
 
+def level_exchange(boxes) -> None:
+    """LevelData<FArrayBox>::exchange() over the LevelBoxes of one level
+    (grhd_level_exchange): ghost cells inside the problem domain take the
+    values of the box that owns them."""
+    lib = L.load()
+    n = len(boxes)
+    arr = (L.Box * n)(*[b.c_box() for b in boxes])
+    ptrs = (C.c_void_p * n)(*[_ptr(b.state).value for b in boxes])
+    strides = (C.c_int64 * n)(*[b.comp_stride() for b in boxes])
+    err = C.create_string_buffer(256)
+    st = lib.grhd_level_exchange(arr, ptrs, strides, n, err, 256, _stream())
+    if st != L.GRHD_OK:
+        cls = L.InvalidArgument if st == L.GRHD_ERR_INVALID_ARG \
+            else L.GRHDError
+        e = cls(st, None)
+        e.args = (err.value.decode(),)
+        raise e
+
+
 def kitp_config(**kw) -> L.KitpConfig:
     """The disk driver's source-term settings (SimulationConfig,
     Main_GRHDLevelDataBinaryPNKITPDisk.cpp:63-71 defaults) with

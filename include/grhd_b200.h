@@ -403,6 +403,18 @@ int grhd_disk_diagnostics(grhd_ctx *ctx, const double *state,
                           int64_t state_comp_stride, const grhd_box *box,
                           double time, double out[7], void *stream);
 
+/* LevelData<FArrayBox>::exchange() of one level on the device (the
+ * reference calls it before every RHS, FixedBGFArrayBoxFiniteVolume.hpp:
+ * 322-363): every box's ghost cells inside the (non-periodic) problem
+ * domain receive all 11 components from the box whose interior holds
+ * them.  boxes / states / strides: the `count` boxes of the level (a
+ * disjoint layout sharing one domain) and their device states.  Ghosts
+ * outside the domain are left to compute_rhs's outflow fill.  Ordered on
+ * `stream`; err (may be NULL) receives a message on error. */
+int grhd_level_exchange(const grhd_box *boxes, double *const *states,
+                        const int64_t *state_comp_strides, int count,
+                        char *err, int err_cap, void *stream);
+
 /* The header of a KITPCHK1 checkpoint (write_checkpoint /
  * read_checkpoint_header, Examples/GRHDLevelDataBinaryPNKITPDisk/
  * Main_GRHDLevelDataBinaryPNKITPDisk.cpp:1289-1505).  num_components is
