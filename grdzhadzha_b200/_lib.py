@@ -171,6 +171,9 @@ SIGNATURES = {
     "grhd_advance_ssprk2": (C.c_int, [_vp, _vp, C.c_int64, _P(Box), _dp,
                                       C.c_double, C.c_double,
                                       _P(Diagnostics), _vp]),
+    "grhd_ssprk2_stage": (C.c_int, [_vp, C.c_int, _vp, C.c_int64, _vp,
+                                    C.c_int64, _P(Box), _dp, C.c_double,
+                                    C.c_double, _P(Diagnostics), _vp]),
     "grhd_advance_rk4": (C.c_int, [_vp, _vp, C.c_int64, _P(Box), _dp,
                                    C.c_double, C.c_double, _P(Diagnostics),
                                    _vp]),
@@ -216,6 +219,8 @@ SIGNATURES = {
     "grhd_level_exchange": (C.c_int, [_P(Box), _P(C.c_void_p),
                                       _P(C.c_int64), C.c_int, C.c_char_p,
                                       C.c_int, _vp]),
+    "grhd_region_copy": (C.c_int, [C.c_int, _vp, C.c_int64, _P(Box),
+                                   _P(C.c_int), _P(C.c_int), _vp, _vp]),
     "grhd_checkpoint_write": (C.c_int, [C.c_char_p, _P(CheckpointHeader),
                                         C.c_char_p, _vp, C.c_int64, _P(Box),
                                         C.c_char_p, C.c_int, _vp]),

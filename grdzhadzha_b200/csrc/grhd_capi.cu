@@ -825,6 +825,40 @@ void enqueue_rk4_any(grhd_ctx *ctx, double *state, const BoxDev &b,
         enqueue_rk4<double>(ctx, state, b, inverse_dx, time, dt, want_cfl, s);
 }
 
+// advance_ssprk2 (:563-589) cut at its two RHS evaluations, for a level
+// whose ghosts the caller exchanges in between: stage 1 stage_state =
+// state + dt L(state), recovered at t + dt; stage 2 state = (state +
+// stage_state + dt L(stage_state)) / 2 (combine_ssprk2_conserved_state),
+// recovered.  The same kernels as the fused single-box step, without the
+// fusion of the stage with the next RHS's per-cell pass.
+template <typename T>
+void enqueue_ssprk2_stage(grhd_ctx *ctx, int stage, double *state,
+                          const BoxDev &b, double *stage_state,
+                          const BoxDev &sb, const Background &bg0,
+                          const Background &bg1, const double inverse_dx[3],
+                          double dt, cudaStream_t s)
+{
+    T *k = scratch<T>(ctx->kbuf), *prim = scratch<T>(ctx->prim),
+      *src = scratch<T>(ctx->src);
+    if (stage == 1)
+    {
+        enqueue_rhs<T>(ctx, k, state, b, bg0, inverse_dx, s, false, 0.5 * dt);
+        Timed t_(ctx, GRHD_K_STAGE, s);
+        launch_stage<T>(1, state, b.cs, nullptr, 0, stage_state, sb.cs, k,
+                        nullptr, prim, src, false, b, bg1, ctx->opt, 0, dt,
+                        false, inverse_dx, ctx->status, s);
+    }
+    else
+    {
+        enqueue_rhs<T>(ctx, k, stage_state, sb, bg1, inverse_dx, s, false,
+                       0.5 * dt);
+        Timed t_(ctx, GRHD_K_STAGE, s);
+        launch_stage<T>(2, state, b.cs, stage_state, sb.cs, state, b.cs, k,
+                        nullptr, prim, nullptr, false, b, bg1, ctx->opt, 0, dt,
+                        false, inverse_dx, ctx->status, s);
+    }
+}
+
 } // namespace
 
 extern "C" {
@@ -844,6 +878,40 @@ int grhd_advance_ssprk2(grhd_ctx *ctx, double *state, int64_t state_cs,
     else
         enqueue_ssprk2<double>(ctx, state, b, inverse_dx, time, dt, s);
     st = finish_status(ctx, b, state, make_background(ctx->params, time), s);
+    read_diag(ctx, diag);
+    return st;
+}
+
+int grhd_ssprk2_stage(grhd_ctx *ctx, int stage, double *state,
+                      int64_t state_cs, double *stage_state,
+                      int64_t stage_cs, const grhd_box *box,
+                      const double inverse_dx[3], double time, double dt,
+                      grhd_diagnostics *diag, void *stream)
+{
+    int st = common_checks(ctx, state, box);
+    if (st)
+        return st;
+    if (!stage_state || !inverse_dx || (stage != 1 && stage != 2))
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "ssprk2 stage is 1 or 2 and needs a stage state and "
+                         "inverse_dx");
+    cudaStream_t s = (cudaStream_t)stream;
+    const BoxDev b = make_box(box, state_cs);
+    const BoxDev sb = make_box(box, stage_cs);
+    if ((st = check_strides(ctx, b, state_cs, -1)) ||
+        (st = check_strides(ctx, sb, stage_cs, -1)) ||
+        (st = ensure_scratch(ctx, b, false)) || (st = reset_status(ctx, s)))
+        return st;
+    const Background bg0 = make_background(ctx->params, time);
+    const Background bg1 = make_background(ctx->params, time + dt);
+    if (ctx->params.precision == GRHD_PRECISION_MIXED)
+        enqueue_ssprk2_stage<float>(ctx, stage, state, b, stage_state, sb,
+                                    bg0, bg1, inverse_dx, dt, s);
+    else
+        enqueue_ssprk2_stage<double>(ctx, stage, state, b, stage_state, sb,
+                                     bg0, bg1, inverse_dx, dt, s);
+    st = stage == 1 ? finish_status(ctx, b, state, bg0, s)
+                    : finish_status(ctx, sb, stage_state, bg1, s);
     read_diag(ctx, diag);
     return st;
 }
@@ -1426,6 +1494,22 @@ int grhd_level_exchange(const grhd_box *boxes, double *const *states,
     if (e != cudaSuccess)
         return io_error(err, err_cap, cudaGetErrorString(e), GRHD_ERR_CUDA);
     return GRHD_OK;
+}
+
+int grhd_region_copy(int pack, double *state, int64_t state_cs,
+                     const grhd_box *box, const int lo[3], const int hi[3],
+                     double *buffer, void *stream)
+{
+    if (!state || !buffer || !lo || !hi || !valid_box(box))
+        return GRHD_ERR_INVALID_ARG;
+    const BoxDev b = make_box(box, state_cs);
+    if (state_cs < b.gvol())
+        return GRHD_ERR_INVALID_ARG;
+    for (int d = 0; d < 3; ++d)
+        if (lo[d] > hi[d] || lo[d] < b.glo[d] || hi[d] > b.ghi[d])
+            return GRHD_ERR_INVALID_ARG;
+    launch_region(pack != 0, state, b, buffer, lo, hi, (cudaStream_t)stream);
+    return cudaGetLastError() == cudaSuccess ? GRHD_OK : GRHD_ERR_CUDA;
 }
 
 int grhd_checkpoint_write(const char *path, const grhd_checkpoint_header *h,

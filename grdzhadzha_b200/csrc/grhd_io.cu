@@ -137,6 +137,32 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// One region [lo, lo + n) of the ghosted box to / from a packed buffer
+// [component][k][j][i] (halo messages between ranks).
+template <bool PACK>
+__global__ void __launch_bounds__(256)
+    k_region(double *__restrict__ state, BoxDev b, double *__restrict__ buf,
+             int lo0, int lo1, int lo2, int n0, int n1, int n2)
+{
+    const int64_t n = (int64_t)n0 * n1 * n2;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int i = lo0 + (int)(t % n0);
+        const int64_t r = t / n0;
+        const int j = lo1 + (int)(r % n1);
+        const int k = lo2 + (int)(r / n1);
+        const int64_t g = b.gidx(i, j, k);
+        for (int c = 0; c < kStateComps; ++c)
+        {
+            if (PACK)
+                buf[c * n + t] = state[c * b.cs + g];
+            else
+                state[c * b.cs + g] = buf[c * n + t];
+        }
+    }
+}
+
 int grid_of(int64_t n)
 {
     int64_t g = (n + 255) / 256;
@@ -177,6 +203,20 @@ void launch_copy_region(double *dst, const BoxDev &db, const double *src,
               n2 = hi[2] - lo[2] + 1;
     k_copy_region<<<grid_of((int64_t)n0 * n1 * n2), 256, 0, s>>>(
         dst, db, src, sb, lo[0], lo[1], lo[2], n0, n1, n2);
+}
+
+void launch_region(bool pack, double *state, const BoxDev &b, double *buf,
+                   const int lo[3], const int hi[3], cudaStream_t s)
+{
+    const int n0 = hi[0] - lo[0] + 1, n1 = hi[1] - lo[1] + 1,
+              n2 = hi[2] - lo[2] + 1;
+    const int g = grid_of((int64_t)n0 * n1 * n2);
+    if (pack)
+        k_region<true><<<g, 256, 0, s>>>(state, b, buf, lo[0], lo[1], lo[2],
+                                         n0, n1, n2);
+    else
+        k_region<false><<<g, 256, 0, s>>>(state, b, buf, lo[0], lo[1], lo[2],
+                                          n0, n1, n2);
 }
 
 } // namespace grhd

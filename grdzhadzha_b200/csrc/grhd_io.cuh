@@ -39,4 +39,9 @@ void launch_copy_region(double *dst, const BoxDev &db, const double *src,
                         const BoxDev &sb, const int lo[3], const int hi[3],
                         cudaStream_t s);
 
+// The 11 components of the region [lo, hi] (inside the ghosted box) into
+// (pack) or out of a packed buffer [component][k][j][i].
+void launch_region(bool pack, double *state, const BoxDev &b, double *buf,
+                   const int lo[3], const int hi[3], cudaStream_t s);
+
 } // namespace grhd

@@ -321,6 +321,36 @@ class _OperatorBase:
                        C.byref(d), _stream()))
         return d
 
+    def ssprk2_stage(self, stage, state: LevelBox, stage_state: LevelBox,
+                     dt, inverse_dx_U=None, time=0.0):
+        """One of the two halves of advance_ssprk2 (:563-589) for a level
+        whose ghosts the caller exchanges before each (grhd_ssprk2_stage):
+        1: stage_state = state + dt L(state); 2: state = (state +
+        stage_state + dt L(stage_state)) / 2; each recovered."""
+        if tuple(stage_state.lo) != tuple(state.lo) or \
+                tuple(stage_state.hi) != tuple(state.hi):
+            raise ValueError("state and stage state cover different boxes")
+        d = L.Diagnostics()
+        b = state.c_box()
+        self._check(self._lib.grhd_ssprk2_stage(
+            self._ctx, int(stage), _ptr(state.state), state.comp_stride(),
+            _ptr(stage_state.state), stage_state.comp_stride(), C.byref(b),
+            self._inv(inverse_dx_U), time, dt, C.byref(d), _stream()))
+        return d
+
+    def advance_level_ssprk2(self, boxes, stage_boxes, dt, inverse_dx_U=None,
+                             time=0.0):
+        """advance_ssprk2 of a level of several boxes on this device: the
+        reference's sequence (:563-589) with LevelData::exchange() before
+        each RHS (grhd_level_exchange).  stage_boxes: one scratch LevelBox
+        per box, same boxes."""
+        level_exchange(boxes)
+        for b, sb in zip(boxes, stage_boxes):
+            self.ssprk2_stage(1, b, sb, dt, inverse_dx_U, time)
+        level_exchange(stage_boxes)
+        for b, sb in zip(boxes, stage_boxes):
+            self.ssprk2_stage(2, b, sb, dt, inverse_dx_U, time)
+
     # ---- initial data (FixedBGTorus.hpp, Michel test) ----
 
     def fill_torus(self, state: LevelBox, inner_radius, pressure_max_radius,

@@ -221,6 +221,19 @@ int grhd_advance_ssprk2(grhd_ctx *ctx, double *state,
                         const double inverse_dx[3], double time, double dt,
                         grhd_diagnostics *diag, void *stream);
 
+/* advance_ssprk2 (:563-589 / :782-809) cut at its two RHS evaluations, for
+ * a level of several boxes or ranks whose ghosts the caller exchanges
+ * before each stage (the reference's compute_rhs exchanges inside):
+ *   stage 1: stage_state = state + dt L(state), recovered at time + dt;
+ *   stage 2: state = (state + stage_state + dt L(stage_state)) / 2
+ *            (combine_ssprk2_conserved_state), recovered.
+ * state and stage_state are ghosted states of the same box. */
+int grhd_ssprk2_stage(grhd_ctx *ctx, int stage, double *state,
+                      int64_t state_comp_stride, double *stage_state,
+                      int64_t stage_comp_stride, const grhd_box *box,
+                      const double inverse_dx[3], double time, double dt,
+                      grhd_diagnostics *diag, void *stream);
+
 /* New (no reference counterpart; the reference integrates with SSPRK2
  * only): classic four-stage RK4 with the reference's post-update recovery
  * after every stage, stage times t, t+dt/2, t+dt/2, t+dt. */
@@ -414,6 +427,15 @@ int grhd_disk_diagnostics(grhd_ctx *ctx, const double *state,
 int grhd_level_exchange(const grhd_box *boxes, double *const *states,
                         const int64_t *state_comp_strides, int count,
                         char *err, int err_cap, void *stream);
+
+/* The halo message of a level split over ranks (LevelData::exchange()
+ * across MPI ranks in the reference): the 11 components of the cells
+ * [lo, hi] (inside the ghosted box) into a packed device buffer laid out
+ * [component][k][j][i] (pack != 0), or from it into the state (pack == 0).
+ * Ordered on `stream`. */
+int grhd_region_copy(int pack, double *state, int64_t state_comp_stride,
+                     const grhd_box *box, const int lo[3], const int hi[3],
+                     double *buffer, void *stream);
 
 /* The header of a KITPCHK1 checkpoint (write_checkpoint /
  * read_checkpoint_header, Examples/GRHDLevelDataBinaryPNKITPDisk/

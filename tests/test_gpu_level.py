@@ -161,3 +161,120 @@ def test_exchange_rejects_overlapping_boxes():
                    domain_hi=(7, 7, 7))
     with pytest.raises(G.InvalidArgument, match="overlap"):
         G.level_exchange([a, b])
+
+
+def _split_stage(parts):
+    import grdzhadzha_b200 as G
+    return [G.LevelBox(lo=lv.lo, hi=lv.hi, ghost=2, domain_lo=lv.domain_lo,
+                       domain_hi=lv.domain_hi,
+                       state=torch.full_like(lv.state, float("nan")))
+            for lv in parts]
+
+
+def _gather(box, parts):
+    z, y, x = [box.hi[d] - box.lo[d] + 1 for d in (2, 1, 0)]
+    out = torch.empty((11, z, y, x), dtype=torch.float64, device="cuda")
+    for lv in parts:
+        out[(slice(None),) + _interior_slice(box, lv.lo, lv.hi)] = \
+            lv.interior()
+    return out
+
+
+SSPRK2_TOL = 1e-12
+
+
+@pytest.mark.parametrize("name", ["ksdisk", "pndisk", "torus_a09"])
+def test_cut_level_ssprk2(name):
+    """advance_ssprk2 of the cut level (exchange before each RHS,
+    grhd_ssprk2_stage per box) against the single box's fused
+    grhd_advance_ssprk2, three steps: <= 1e-12 of each component's scale
+    (the split stage runs the per-cell pass of the stage RHS as its own
+    kernel instead of fused into the update; same arithmetic; measured on
+    B200: 0 to 7e-16)."""
+    p, box, s, t = cases.CASES[name]()
+    op = cases.gpu_operator(p)
+    single = cases.gpu_level(box, s)
+    dt = op.compute_stable_dt(single, cfl=0.3, time=t)
+    parts = _split_level(box, s, CUTS[name])
+    stages = _split_stage(parts)
+    for n in range(3):
+        op.advance_ssprk2(single, time=t + n * dt, dt=dt)
+        op.advance_level_ssprk2(parts, stages, dt, time=t + n * dt)
+    ref = single.interior().cpu().numpy().reshape(11, -1)
+    got = _gather(box, parts).cpu().numpy().reshape(11, -1)
+    err = cases.rel_err(got[:5], ref[:5])
+    print(f"{name} ssprk2 {len(parts)} boxes: state err {err}")
+    assert np.all(err <= SSPRK2_TOL), err
+
+
+@pytest.mark.parametrize("layout", ["slabs", "pencils"])
+def test_distributed_level_virtual_ranks(layout):
+    """The multi-rank level (grdzhadzha_b200.halo) with its ranks driven in
+    one process through a LocalTransport: device pack / unpack of the
+    halos (grhd_region_copy), the RHS of each rank's box and three SSPRK2
+    steps, against the single box."""
+    import grdzhadzha_b200 as G
+    from grdzhadzha_b200 import halo as H
+    p, box, s, t = cases.CASES["torus_a09"]()
+    op = cases.gpu_operator(p)
+    dlo, dhi = tuple(box.dlo), tuple(box.dhi)
+    boxes = (H.slab_boxes(dlo, dhi, 5) if layout == "slabs"
+             else H.pencil_boxes(dlo, dhi, 3, 2))
+    mailbox = {}
+    ranks = [H.DistributedLevel(op, boxes, r, dlo, dhi,
+                                transport=H.LocalTransport(mailbox, r))
+             for r in range(len(boxes))]
+    full = _split_level(box, s, [[], [], []])[0]
+    parts = _split_level(box, s, [[], [], []])
+    for lv in ranks:
+        src = _split_level_box(box, s, lv.state.lo, lv.state.hi)
+        lv.state.state.copy_(src.state)
+        assert lv.halo.sends and lv.halo.recvs
+    for lv in ranks:
+        lv.halo.begin(lv.state)
+    for lv in ranks:
+        lv.halo.end(lv.state)
+    assert not mailbox
+    rhs1 = full.new_rhs()
+    op.compute_rhs(rhs1, full, time=t)
+    rhs_n = torch.empty_like(rhs1)
+    for lv in ranks:
+        assert not torch.isnan(lv.state.state).any()
+        r = lv.state.new_rhs()
+        op.compute_rhs(r, lv.state, time=t)
+        rhs_n[(slice(None),) + _interior_slice(box, lv.state.lo,
+                                               lv.state.hi)] = r
+    err = cases.rel_err(rhs_n.cpu().numpy().reshape(5, -1),
+                        rhs1.cpu().numpy().reshape(5, -1))
+    assert np.all(err <= 1e-13), err
+    single = parts[0]
+    dt = op.compute_stable_dt(single, cfl=0.3, time=t)
+    inv = max(lv.local_max_inverse_dt(time=t) for lv in ranks)
+    assert abs(0.3 / inv - dt) <= 1e-14 * dt
+    for n in range(3):
+        op.advance_ssprk2(single, time=t + n * dt, dt=dt)
+        H.advance_local_ssprk2(ranks, dt, time=t + n * dt)
+    ref = single.interior().cpu().numpy().reshape(11, -1)
+    got = _gather(box, [lv.state for lv in ranks]).cpu().numpy()
+    err = cases.rel_err(got.reshape(11, -1)[:5], ref[:5])
+    print(f"{layout} {len(ranks)} virtual ranks: state err {err}")
+    assert np.all(err <= SSPRK2_TOL), err
+
+
+def _split_level_box(box, s, lo, hi):
+    """One box of the cut level with its in-domain ghosts poisoned."""
+    cuts = [[c for c in (lo[d], hi[d] + 1) if box.lo[d] < c <= box.hi[d]]
+            for d in range(3)]
+    for lv in _split_level(box, s, cuts):
+        if tuple(lv.lo) == tuple(lo):
+            return lv
+    raise AssertionError("box not found")
+
+
+def test_region_copy_rejects_outside_regions():
+    from grdzhadzha_b200 import halo as H
+    import grdzhadzha_b200 as G
+    lv = G.LevelBox(lo=(0, 0, 0), hi=(3, 3, 3))
+    buf = torch.empty(11 * 64, dtype=torch.float64, device="cuda")
+    with pytest.raises(G.InvalidArgument):
+        H.DeviceRegions().pack(lv, (0, 0, 0), (3, 3, 6), buf)
