@@ -7,6 +7,7 @@ from .operator import (  # noqa: F401
     IdealGasEOS,
     KerrSchild,
     LevelBox,
+    LevelDataFiniteVolumeOperator,
     RecoveryOptions,
     TimeDependentFixedBGLevelDataFiniteVolumeOperator,
     level_exchange,

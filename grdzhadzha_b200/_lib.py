@@ -219,6 +219,17 @@ SIGNATURES = {
     "grhd_level_exchange": (C.c_int, [_P(Box), _P(C.c_void_p),
                                       _P(C.c_int64), C.c_int, C.c_char_p,
                                       C.c_int, _vp]),
+    "grhd_ccz4_compute_rhs": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_int64,
+                                        _P(Box), _dp, _vp]),
+    "grhd_ccz4_recover_primitives": (C.c_int, [_vp, _vp, C.c_int64, _P(Box),
+                                               _P(Diagnostics), _vp]),
+    "grhd_ccz4_update_conserved": (C.c_int, [_vp, _vp, C.c_int64, _vp,
+                                             C.c_int64, _P(Box), C.c_double,
+                                             C.c_int, _P(Diagnostics), _vp]),
+    "grhd_ccz4_compute_max_inverse_dt": (C.c_int, [_vp, _vp, C.c_int64,
+                                                   _P(Box), _dp, _dp, _vp]),
+    "grhd_ccz4_advance_ssprk2": (C.c_int, [_vp, _vp, C.c_int64, _P(Box), _dp,
+                                           C.c_double, _P(Diagnostics), _vp]),
     "grhd_region_copy": (C.c_int, [C.c_int, _vp, C.c_int64, _P(Box),
                                    _P(C.c_int), _P(C.c_int), _vp, _vp]),
     "grhd_checkpoint_write": (C.c_int, [C.c_char_p, _P(CheckpointHeader),

@@ -35,6 +35,10 @@ struct grhd_ctx
     size_t int_cap = 0;      // doubles per interior buffer
     double *stage = nullptr; // 11 comps over the ghosted box
     size_t stage_cap = 0;
+    double *ccz4_geo = nullptr;   // CCZ4 operator: geometry cache (16 comps)
+    size_t ccz4_geo_cap = 0;
+    double *ccz4_stage = nullptr; // CCZ4 operator: SSPRK2 stage (36 comps)
+    size_t ccz4_stage_cap = 0;
     double *mdot_part = nullptr; // per face-kernel block accretion sums
     size_t mdot_cap = 0;
     double *mdot_acc = nullptr;  // [Mdot of the last RHS, time integral]
@@ -554,6 +558,8 @@ void grhd_destroy(grhd_ctx *ctx)
     cudaFree(ctx->flag);
     cudaFree(ctx->mdot_part);
     cudaFree(ctx->mdot_acc);
+    cudaFree(ctx->ccz4_geo);
+    cudaFree(ctx->ccz4_stage);
     if (ctx->status_h)
         cudaFreeHost(ctx->status_h);
     for (auto &r : ctx->prof_pending)
@@ -859,9 +865,220 @@ void enqueue_ssprk2_stage(grhd_ctx *ctx, int stage, double *state,
     }
 }
 
+// ---- the operator on CCZ4-stored geometry (LevelDataFiniteVolumeOperator,
+// FArrayBoxFiniteVolume.hpp:1215-1364)
+
+// The device status of a CCZ4 call as the reference's exceptions.
+int ccz4_finish(grhd_ctx *ctx, const BoxDev &b, const double *state,
+                cudaStream_t s)
+{
+    GRHD_CUDA(ctx, cudaGetLastError());
+    GRHD_CUDA(ctx, cudaMemcpyAsync(ctx->status_h, ctx->status,
+                                   sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                                   s));
+    GRHD_CUDA(ctx, cudaStreamSynchronize(s));
+    const unsigned long long key = ctx->status_h->err_key;
+    if (key == kNoError)
+        return GRHD_OK;
+    const int where = (int)(key >> 56);
+    const int64_t order = (int64_t)(key & ((1ull << 56) - 1));
+    int cell[3];
+    if (where == GRHD_WHERE_CFL)
+    {
+        cell[0] = b.lo[0] + (int)(order % b.in[0]);
+        cell[1] = b.lo[1] + (int)((order / b.in[0]) % b.in[1]);
+        cell[2] = b.lo[2] + (int)(order / ((int64_t)b.in[0] * b.in[1]));
+    }
+    else
+    {
+        cell[0] = b.glo[0] + (int)(order % b.gn[0]);
+        cell[1] = b.glo[1] + (int)((order / b.gn[0]) % b.gn[1]);
+        cell[2] = b.glo[2] + (int)(order / ((int64_t)b.gn[0] * b.gn[1]));
+    }
+    double residual = 0.0;
+    launch_ccz4_probe(state, b, ctx->opt, cell[0], cell[1], cell[2],
+                      ctx->probe, s);
+    GRHD_CUDA(ctx, cudaMemcpyAsync(&residual, ctx->probe, sizeof(double),
+                                   cudaMemcpyDeviceToHost, s));
+    GRHD_CUDA(ctx, cudaStreamSynchronize(s));
+    char msg[256];
+    std::snprintf(msg, sizeof(msg),
+                  where == GRHD_WHERE_CFL
+                      ? "GRHD primitive recovery failed at (%d,%d,%d) while "
+                        "computing CFL speed, residual %g"
+                      : "GRHD primitive recovery failed at (%d,%d,%d) with "
+                        "residual %g",
+                  cell[0], cell[1], cell[2], residual);
+    return set_error(ctx, GRHD_ERR_RECOVERY, where, cell, residual, msg);
+}
+
+int ccz4_checks(grhd_ctx *ctx, const double *state, int64_t state_cs,
+                const grhd_box *box, int64_t rhs_cs, BoxDev &b,
+                cudaStream_t s)
+{
+    int st = common_checks(ctx, state, box);
+    if (st)
+        return st;
+    b = make_box(box, state_cs);
+    if ((st = check_strides(ctx, b, state_cs, rhs_cs)) ||
+        (st = ensure_scratch(ctx, b, false)) ||
+        (st = grow(ctx, &ctx->ccz4_geo, &ctx->ccz4_geo_cap,
+                   16 * (size_t)b.gvol())) ||
+        (st = reset_status(ctx, s)))
+        return st;
+    return GRHD_OK;
+}
+
+// compute_leveldata_flux_rhs_from_ccz4_geometry (:1047-1090) on one box:
+// the fills, the ghosted-box recovery into the caches, then one kernel for
+// the three directional flux differences and the sources.
+void enqueue_ccz4_rhs(grhd_ctx *ctx, double *rhs, int64_t rhs_cs,
+                      double *state, const BoxDev &b,
+                      const double inverse_dx[3], cudaStream_t s)
+{
+    launch_ccz4_fill(state, b, true, s);
+    launch_ccz4_cells(state, b, ctx->opt, ctx->prim, ctx->ccz4_geo,
+                      ctx->status, s);
+    launch_ccz4_rhs(state, b, ctx->opt, ctx->prim, ctx->ccz4_geo, rhs, rhs_cs,
+                    inverse_dx, ctx->status, s);
+    ctx->launches += 3;
+}
+
 } // namespace
 
 extern "C" {
+
+int grhd_ccz4_compute_rhs(grhd_ctx *ctx, double *rhs, int64_t rhs_cs,
+                          double *state, int64_t state_cs,
+                          const grhd_box *box, const double inverse_dx[3],
+                          void *stream)
+{
+    if (ctx && (!rhs || !inverse_dx))
+    {
+        std::memset(&ctx->last_error, 0, sizeof(ctx->last_error));
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "null rhs or inverse_dx");
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    BoxDev b;
+    int st = ccz4_checks(ctx, state, state_cs, box, rhs_cs, b, s);
+    if (st)
+        return st;
+    enqueue_ccz4_rhs(ctx, rhs, rhs_cs, state, b, inverse_dx, s);
+    return ccz4_finish(ctx, b, state, s);
+}
+
+int grhd_ccz4_recover_primitives(grhd_ctx *ctx, double *state,
+                                 int64_t state_cs, const grhd_box *box,
+                                 grhd_diagnostics *diag, void *stream)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    BoxDev b;
+    int st = ccz4_checks(ctx, state, state_cs, box, -1, b, s);
+    if (st)
+        return st;
+    launch_ccz4_recover(state, b, ctx->opt, ctx->status, s);
+    ++ctx->launches;
+    st = ccz4_finish(ctx, b, state, s);
+    read_diag(ctx, diag);
+    return st;
+}
+
+int grhd_ccz4_update_conserved(grhd_ctx *ctx, double *state,
+                               int64_t state_cs, const double *rhs,
+                               int64_t rhs_cs, const grhd_box *box, double dt,
+                               int recover, grhd_diagnostics *diag,
+                               void *stream)
+{
+    if (ctx && !rhs)
+    {
+        std::memset(&ctx->last_error, 0, sizeof(ctx->last_error));
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "null rhs");
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    BoxDev b;
+    int st = ccz4_checks(ctx, state, state_cs, box, rhs_cs, b, s);
+    if (st)
+        return st;
+    launch_ccz4_update(state, nullptr, 0, rhs, rhs_cs, b, dt, 0, s);
+    ++ctx->launches;
+    if (recover)
+    {
+        launch_ccz4_recover(state, b, ctx->opt, ctx->status, s);
+        ++ctx->launches;
+    }
+    st = ccz4_finish(ctx, b, state, s);
+    read_diag(ctx, diag);
+    return st;
+}
+
+int grhd_ccz4_compute_max_inverse_dt(grhd_ctx *ctx, const double *state,
+                                     int64_t state_cs, const grhd_box *box,
+                                     const double inverse_dx[3], double *out,
+                                     void *stream)
+{
+    if (ctx && (!out || !inverse_dx))
+    {
+        std::memset(&ctx->last_error, 0, sizeof(ctx->last_error));
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "null output or inverse_dx");
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    BoxDev b;
+    int st = ccz4_checks(ctx, state, state_cs, box, -1, b, s);
+    if (st)
+        return st;
+    launch_ccz4_max_inv_dt(state, b, ctx->opt, inverse_dx, ctx->status, s);
+    ++ctx->launches;
+    st = ccz4_finish(ctx, b, state, s);
+    if (st == GRHD_OK)
+        *out = bits_to_double(ctx->status_h->maxinv_bits);
+    return st;
+}
+
+int grhd_ccz4_advance_ssprk2(grhd_ctx *ctx, double *state, int64_t state_cs,
+                             const grhd_box *box, const double inverse_dx[3],
+                             double dt, grhd_diagnostics *diag, void *stream)
+{
+    if (ctx && (!inverse_dx || !box_is_domain(box)))
+    {
+        std::memset(&ctx->last_error, 0, sizeof(ctx->last_error));
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "advance needs inverse_dx and the box to cover the "
+                         "whole domain");
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    BoxDev b;
+    int st = ccz4_checks(ctx, state, state_cs, box, -1, b, s);
+    if (st)
+        return st;
+    const int64_t gv = b.gvol();
+    if ((st = grow(ctx, &ctx->ccz4_stage, &ctx->ccz4_stage_cap,
+                   (size_t)GRHD_CCZ4_NUM_VARS * gv)))
+        return st;
+    BoxDev sb = b;
+    sb.cs = gv;
+    double *stage = ctx->ccz4_stage;
+    double *k0 = ctx->kbuf, *k1 = ctx->src; // rhs_initial, rhs_stage
+    // advance_ssprk2 (:1323-1348): stage = state; rhs_initial = L(state);
+    // stage += dt rhs_initial, recovered; rhs_stage = L(stage);
+    // state = (state + stage + dt rhs_stage) / 2, recovered
+    GRHD_CUDA(ctx, cudaMemcpy2DAsync(stage, gv * sizeof(double), state,
+                                     state_cs * sizeof(double),
+                                     gv * sizeof(double), GRHD_CCZ4_NUM_VARS,
+                                     cudaMemcpyDeviceToDevice, s));
+    enqueue_ccz4_rhs(ctx, k0, b.ivol(), state, b, inverse_dx, s);
+    launch_ccz4_update(stage, nullptr, 0, k0, b.ivol(), sb, dt, 0, s);
+    launch_ccz4_recover(stage, sb, ctx->opt, ctx->status, s);
+    enqueue_ccz4_rhs(ctx, k1, b.ivol(), stage, sb, inverse_dx, s);
+    launch_ccz4_update(state, stage, gv, k1, b.ivol(), b, dt, 1, s);
+    launch_ccz4_recover(state, b, ctx->opt, ctx->status, s);
+    ctx->launches += 4;
+    st = ccz4_finish(ctx, b, state, s);
+    read_diag(ctx, diag);
+    return st;
+}
 
 int grhd_advance_ssprk2(grhd_ctx *ctx, double *state, int64_t state_cs,
                         const grhd_box *box, const double inverse_dx[3],

@@ -1672,6 +1672,410 @@ template <typename T> size_t faces_smem()
            (5 * kPW * kPW + 2 * kGeoFields * kGW * kGW + 2 * 5 * kTB * kTC);
 }
 
+// ---------------------------------------------- CCZ4-stored geometry
+// LevelDataFiniteVolumeOperator (Source/Matter/GRHD/FArrayBoxFiniteVolume.hpp:
+// 1215-1364): the same Valencia operator with the geometry of every cell
+// read from GRChombo's CCZ4 variables of the state (chi, h_ij, A_ij, K,
+// lapse, shift; components 0..24, the GRHD ones from 25) and the metric
+// derivatives of the sources as finite differences.  FP64 only.
+
+constexpr int kCzChi = 0, kCzH = 1, kCzK = 7, kCzA = 8, kCzLapse = 18,
+              kCzShift = 19;
+constexpr int kCzGeoFields = 16; // gLL[6] gUU[6] lapse shift[3]
+
+// load_ccz4_geometry (:168-192): gamma = h / chi, gamma^-1 = chi h^-1 (the
+// symmetric cofactor inverse of GRChombo's TensorAlgebra), K_ij = A_ij /
+// chi + gamma_ij K / 3.
+__device__ __forceinline__ void ccz4_geo(const double *__restrict__ s,
+                                         int64_t cs, int64_t g, Geo &geo,
+                                         double *K)
+{
+    const double chi = s[kCzChi * cs + g];
+    double h[6], hu[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+        h[q] = s[(kCzH + q) * cs + g];
+    const double det = h[0] * h[3] * h[5] + 2 * h[1] * h[2] * h[4] -
+                       h[0] * h[4] * h[4] - h[3] * h[2] * h[2] -
+                       h[5] * h[1] * h[1];
+    hu[0] = (h[3] * h[5] - h[4] * h[4]) / det;
+    hu[1] = (h[2] * h[4] - h[1] * h[5]) / det;
+    hu[2] = (h[1] * h[4] - h[2] * h[3]) / det;
+    hu[3] = (h[0] * h[5] - h[2] * h[2]) / det;
+    hu[4] = (h[1] * h[2] - h[0] * h[4]) / det;
+    hu[5] = (h[0] * h[3] - h[1] * h[1]) / det;
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+    {
+        geo.gLL[q] = h[q] / chi;
+        geo.gUU[q] = chi * hu[q];
+    }
+    if (K)
+    {
+        const double trK = s[kCzK * cs + g];
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+            K[q] = s[(kCzA + q) * cs + g] / chi + geo.gLL[q] * trK / 3.0;
+    }
+    geo.lapse = s[kCzLapse * cs + g];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+        geo.shift[d] = s[(kCzShift + d) * cs + g];
+}
+
+__device__ __forceinline__ void geo_put(double *gc, int64_t n, int64_t g,
+                                        const Geo &v)
+{
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+    {
+        gc[q * n + g] = v.gLL[q];
+        gc[(6 + q) * n + g] = v.gUU[q];
+    }
+    gc[12 * n + g] = v.lapse;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+        gc[(13 + d) * n + g] = v.shift[d];
+}
+
+__device__ __forceinline__ Geo geo_get(const double *__restrict__ gc,
+                                       int64_t n, int64_t g)
+{
+    Geo v;
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+    {
+        v.gLL[q] = gc[q * n + g];
+        v.gUU[q] = gc[(6 + q) * n + g];
+    }
+    v.lapse = gc[12 * n + g];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+        v.shift[d] = gc[(13 + d) * n + g];
+    return v;
+}
+
+__device__ __forceinline__ void ghosted_cell(const BoxDev &b, int64_t t,
+                                             int &i, int &j, int &k)
+{
+    i = b.glo[0] + (int)(t % b.gn[0]);
+    const int64_t r = t / b.gn[0];
+    j = b.glo[1] + (int)(r % b.gn[1]);
+    k = b.glo[2] + (int)(r / b.gn[1]);
+}
+
+// fill_conserved_outflow_boundaries (:484-519) and
+// fill_ccz4_geometry_outflow_boundaries (:430-473): a physical ghost copies
+// the conserved variables (when `conserved`) and chi, h_ij, lapse, shift of
+// its source cell (the box's end in each direction it lies outside in).
+__global__ void __launch_bounds__(256)
+    k_ccz4_fill(double *__restrict__ s, BoxDev b, int conserved)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+         t < b.gvol(); t += (int64_t)gridDim.x * blockDim.x)
+    {
+        int iv[3];
+        ghosted_cell(b, t, iv[0], iv[1], iv[2]);
+        int src[3] = {iv[0], iv[1], iv[2]};
+        bool ghost = false;
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+        {
+            if (iv[d] < b.dlo[d])
+            {
+                ghost = true;
+                src[d] = b.lo[d];
+            }
+            else if (iv[d] > b.dhi[d])
+            {
+                ghost = true;
+                src[d] = b.hi[d];
+            }
+        }
+        if (!ghost)
+            continue;
+        const int64_t g = t, sg = b.gidx(src[0], src[1], src[2]);
+        if (conserved)
+            for (int c = 0; c < 5; ++c)
+                s[(kCcz4GrhdOffset + c) * b.cs + g] =
+                    s[(kCcz4GrhdOffset + c) * b.cs + sg];
+        for (int q = 0; q < 7; ++q) // chi, h
+            s[q * b.cs + g] = s[q * b.cs + sg];
+        for (int q = kCzLapse; q < kCzLapse + 4; ++q) // lapse, shift
+            s[q * b.cs + g] = s[q * b.cs + sg];
+    }
+}
+
+// recover_primitives_from_ccz4_geometry over the ghosted box (:681-702):
+// the primitive cache (rho, p, v) and the geometry cache of every cell.
+__global__ void __launch_bounds__(256)
+    k_ccz4_cells(const double *__restrict__ s, BoxDev b, Options o,
+                 double *__restrict__ prim, double *__restrict__ gc,
+                 DevStatus *st)
+{
+    const double *q = s + kCcz4GrhdOffset * b.cs;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+         t < b.gvol(); t += (int64_t)gridDim.x * blockDim.x)
+    {
+        Geo geo;
+        ccz4_geo(s, b.cs, t, geo, nullptr);
+        geo_put(gc, b.gvol(), t, geo);
+        Prim pr;
+        if (!con2prim(o, load_cons(q, b.cs, t), geo.gUU, pr, nullptr,
+                      nullptr))
+        {
+            record_error(st, 2, t);
+            pr.rho = pr.p = 1.0;
+            pr.v[0] = pr.v[1] = pr.v[2] = 0.0;
+        }
+        store_pv(prim, b.gvol(), t, pr);
+    }
+}
+
+__device__ __forceinline__ double log_sqrt_det6(const double *g)
+{
+    const double det = g[0] * g[3] * g[5] + 2 * g[1] * g[2] * g[4] -
+                       g[0] * g[4] * g[4] - g[3] * g[2] * g[2] -
+                       g[5] * g[1] * g[1];
+    return (det <= 0.0 || !isfinite(det)) ? 0.0 : 0.5 * log(det);
+}
+
+// The RHS of one interior cell: per direction the two faces of the cell
+// (compute_directional_flux_rhs_from_ccz4_geometry, :784-833, every face
+// twice as the reference computes it), then the static-metric sources with
+// finite-difference derivatives (add_static_metric_sources_to_conserved_rhs,
+// :367-427; one-sided where a neighbour's stored primitives are metric-
+// source atmosphere, make_metric_source_derivative_stencil, :283-322).
+__global__ void __launch_bounds__(256)
+    k_ccz4_rhs(const double *__restrict__ s, BoxDev b, Options o,
+               const double *__restrict__ prim, const double *__restrict__ gc,
+               double *__restrict__ rhs, int64_t rcs, double inv0,
+               double inv1, double inv2, DevStatus *st)
+{
+    const int64_t n = b.gvol();
+    const double *q = s + kCcz4GrhdOffset * b.cs;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+         t < b.ivol(); t += (int64_t)gridDim.x * blockDim.x)
+    {
+        int i, j, k;
+        interior_cell(b, t, i, j, k);
+        const int64_t g = b.gidx(i, j, k);
+        const double inv[3] = {inv0, inv1, inv2};
+        const int64_t step[3] = {1, (int64_t)b.gn[0],
+                                 (int64_t)b.gn[0] * b.gn[1]};
+        Cons r;
+        r.D = r.tau = 0.0;
+        r.S[0] = r.S[1] = r.S[2] = 0.0;
+        for (int d = 0; d < 3; ++d)
+        {
+            const int64_t so = step[d];
+            Cons f[2];
+            for (int side = 0; side < 2; ++side)
+            {
+                const int64_t L = g - so + side * so, R = L + so;
+                Geo gf;
+                average_geo(geo_get(gc, n, L), geo_get(gc, n, R), gf);
+                f[side] = face_flux(o, load_pv_global<double>(prim, n, L - so),
+                                    load_pv_global<double>(prim, n, L),
+                                    load_pv_global<double>(prim, n, R),
+                                    load_pv_global<double>(prim, n, R + so),
+                                    gf, d);
+            }
+            r.D += -inv[d] * (f[1].D - f[0].D);
+            r.tau += -inv[d] * (f[1].tau - f[0].tau);
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+                r.S[m] += -inv[d] * (f[1].S[m] - f[0].S[m]);
+        }
+        if (o.use_src)
+        {
+            GeoFull fg;
+            ccz4_geo(s, b.cs, g, fg.g, fg.K);
+            const PV pv = load_pv_global<double>(prim, n, g);
+            Prim pr;
+            pr.rho = pv.q[0];
+            pr.p = pv.q[1];
+            pr.v[0] = pv.q[2];
+            pr.v[1] = pv.q[3];
+            pr.v[2] = pv.q[4];
+            floors(o, pr, fg.g.gLL);
+            if (!is_atmo(o, pr, o.src_atmo_factor))
+            {
+                for (int d = 0; d < 3; ++d)
+                {
+                    fg.dlapse[d] = fg.dlnsqrtg[d] = 0.0;
+#pragma unroll
+                    for (int q6 = 0; q6 < 6; ++q6)
+                        fg.dgamma[d][q6] = 0.0;
+#pragma unroll
+                    for (int m = 0; m < 3; ++m)
+                        fg.dshift[m][d] = 0.0;
+                    const int64_t lo_i = g - step[d], hi_i = g + step[d];
+                    Prim pl, pu;
+                    pl.rho = q[kRho * b.cs + lo_i];
+                    pl.p = q[kPress * b.cs + lo_i];
+                    pu.rho = q[kRho * b.cs + hi_i];
+                    pu.p = q[kPress * b.cs + hi_i];
+                    const bool la = !is_atmo(o, pl, o.src_atmo_factor);
+                    const bool ua = !is_atmo(o, pu, o.src_atmo_factor);
+                    int64_t lc, uc;
+                    double coef;
+                    if (la && ua)
+                    {
+                        lc = lo_i;
+                        uc = hi_i;
+                        coef = 0.5 * inv[d];
+                    }
+                    else if (ua)
+                    {
+                        lc = g;
+                        uc = hi_i;
+                        coef = inv[d];
+                    }
+                    else if (la)
+                    {
+                        lc = lo_i;
+                        uc = g;
+                        coef = inv[d];
+                    }
+                    else
+                        continue;
+                    const Geo gu = geo_get(gc, n, uc), gl = geo_get(gc, n, lc);
+                    fg.dlapse[d] = coef * (gu.lapse - gl.lapse);
+                    fg.dlnsqrtg[d] =
+                        coef * (log_sqrt_det6(gu.gLL) - log_sqrt_det6(gl.gLL));
+#pragma unroll
+                    for (int q6 = 0; q6 < 6; ++q6)
+                        fg.dgamma[d][q6] = coef * (gu.gLL[q6] - gl.gLL[q6]);
+#pragma unroll
+                    for (int m = 0; m < 3; ++m)
+                        fg.dshift[m][d] = coef * (gu.shift[m] - gl.shift[m]);
+                }
+                const Cons c = load_cons(q, b.cs, g);
+                const Cons src = static_sources(pr, c, fg);
+                r.D += src.D;
+                r.tau += src.tau;
+#pragma unroll
+                for (int m = 0; m < 3; ++m)
+                    r.S[m] += src.S[m];
+            }
+        }
+        rhs[0 * rcs + t] = r.D;
+        rhs[1 * rcs + t] = r.S[0];
+        rhs[2 * rcs + t] = r.S[1];
+        rhs[3 * rcs + t] = r.S[2];
+        rhs[4 * rcs + t] = r.tau;
+    }
+}
+
+// recover_primitives_and_apply_atmosphere_from_ccz4_geometry (:713-761).
+__global__ void __launch_bounds__(256)
+    k_ccz4_recover(double *__restrict__ s, BoxDev b, Options o, DevStatus *st)
+{
+    double *q = s + kCcz4GrhdOffset * b.cs;
+    unsigned long long cnt[4] = {0, 0, 0, 0};
+    const int64_t n = b.ivol();
+    const int64_t n_pad = (n + blockDim.x - 1) / blockDim.x * blockDim.x;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_pad;
+         t += (int64_t)gridDim.x * blockDim.x)
+    {
+        if (t < n)
+        {
+            int i, j, k;
+            interior_cell(b, t, i, j, k);
+            const int64_t g = b.gidx(i, j, k);
+            Geo geo;
+            ccz4_geo(s, b.cs, g, geo, nullptr);
+            recover_cell(o, geo, load_cons(q, b.cs, g), q, b.cs, g, cnt);
+        }
+        flush_counts(st, cnt);
+        cnt[0] = cnt[1] = cnt[2] = cnt[3] = 0;
+    }
+}
+
+// compute_max_inverse_dt_from_ccz4_geometry (:1139-1183).
+__global__ void __launch_bounds__(256)
+    k_ccz4_max_inv_dt(const double *__restrict__ s, BoxDev b, Options o,
+                      double inv0, double inv1, double inv2, DevStatus *st)
+{
+    const double *q = s + kCcz4GrhdOffset * b.cs;
+    const int64_t n = b.ivol();
+    const int64_t n_pad = (n + blockDim.x - 1) / blockDim.x * blockDim.x;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_pad;
+         t += (int64_t)gridDim.x * blockDim.x)
+    {
+        double cell = 0.0;
+        if (t < n)
+        {
+            int i, j, k;
+            interior_cell(b, t, i, j, k);
+            const int64_t g = b.gidx(i, j, k);
+            Geo geo;
+            ccz4_geo(s, b.cs, g, geo, nullptr);
+            Prim pr;
+            if (!con2prim(o, load_cons(q, b.cs, g), geo.gUU, pr, nullptr,
+                          nullptr))
+                record_error(st, 4, t); // GRHD_WHERE_CFL
+            else
+            {
+                floors(o, pr, geo.gLL);
+                if (!is_atmo(o, pr, 1.0 + 1.0e-12))
+                {
+                    const double inv[3] = {inv0, inv1, inv2};
+                    for (int d = 0; d < 3; ++d)
+                    {
+                        double lo, hi;
+                        char_speeds(o, pr, geo, d, lo, hi);
+                        cell += fmax(fabs(lo), fabs(hi)) * inv[d];
+                    }
+                }
+            }
+        }
+        flush_max(st, cell);
+    }
+}
+
+// add_scaled_conserved_rhs (:927-940) and combine_ssprk2_conserved_state
+// (:942-969) on the GRHD components: mode 0 s += dt rhs; mode 1
+// s = (s + u1 + dt rhs) / 2.
+__global__ void __launch_bounds__(256)
+    k_ccz4_update(double *__restrict__ s, const double *__restrict__ u1,
+                  int64_t ucs, const double *__restrict__ rhs, int64_t rcs,
+                  BoxDev b, double dt, int mode)
+{
+    double *q = s + kCcz4GrhdOffset * b.cs;
+    const double *u = u1 ? u1 + kCcz4GrhdOffset * ucs : nullptr;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+         t < b.ivol(); t += (int64_t)gridDim.x * blockDim.x)
+    {
+        int i, j, k;
+        interior_cell(b, t, i, j, k);
+        const int64_t g = b.gidx(i, j, k);
+        for (int c = 0; c < 5; ++c)
+        {
+            const double x = rhs[c * rcs + t];
+            if (mode == 0)
+                q[c * b.cs + g] += dt * x;
+            else
+                q[c * b.cs + g] = 0.5 * (q[c * b.cs + g] + u[c * ucs + g] +
+                                         dt * x);
+        }
+    }
+}
+
+__global__ void k_ccz4_probe(const double *__restrict__ s, BoxDev b,
+                             Options o, int i, int j, int k, double *out)
+{
+    const int64_t g = b.gidx(i, j, k);
+    Geo geo;
+    ccz4_geo(s, b.cs, g, geo, nullptr);
+    Prim pr;
+    double res = 0.0;
+    con2prim(o, load_cons(s + kCcz4GrhdOffset * b.cs, b.cs, g), geo.gUU, pr,
+             nullptr, &res);
+    *out = res;
+}
+
 } // namespace
 
 cudaError_t configure_kernels()
@@ -1872,6 +2276,58 @@ void launch_eval_con2prim(int64_t n, const double *cons, const double *gUU,
     k_eval_con2prim<<<(int)((n + 127) / 128), 128, 0, s>>>(n, cons, gUU, o,
                                                            prim, ok, iters,
                                                            resid);
+}
+
+void launch_ccz4_fill(double *s, const BoxDev &b, bool conserved,
+                      cudaStream_t st)
+{
+    k_ccz4_fill<<<grid_for(b.gvol(), 256), 256, 0, st>>>(s, b,
+                                                          conserved ? 1 : 0);
+}
+
+void launch_ccz4_cells(const double *s, const BoxDev &b, const Options &o,
+                       double *prim, double *gc, DevStatus *st,
+                       cudaStream_t stream)
+{
+    k_ccz4_cells<<<grid_for(b.gvol(), 256), 256, 0, stream>>>(s, b, o, prim,
+                                                               gc, st);
+}
+
+void launch_ccz4_rhs(const double *s, const BoxDev &b, const Options &o,
+                     const double *prim, const double *gc, double *rhs,
+                     int64_t rcs, const double inv[3], DevStatus *st,
+                     cudaStream_t stream)
+{
+    k_ccz4_rhs<<<grid_for(b.ivol(), 256), 256, 0, stream>>>(
+        s, b, o, prim, gc, rhs, rcs, inv[0], inv[1], inv[2], st);
+}
+
+void launch_ccz4_recover(double *s, const BoxDev &b, const Options &o,
+                         DevStatus *st, cudaStream_t stream)
+{
+    k_ccz4_recover<<<grid_for(b.ivol(), 256), 256, 0, stream>>>(s, b, o, st);
+}
+
+void launch_ccz4_max_inv_dt(const double *s, const BoxDev &b,
+                            const Options &o, const double inv[3],
+                            DevStatus *st, cudaStream_t stream)
+{
+    k_ccz4_max_inv_dt<<<grid_for(b.ivol(), 256), 256, 0, stream>>>(
+        s, b, o, inv[0], inv[1], inv[2], st);
+}
+
+void launch_ccz4_update(double *s, const double *u1, int64_t ucs,
+                        const double *rhs, int64_t rcs, const BoxDev &b,
+                        double dt, int mode, cudaStream_t stream)
+{
+    k_ccz4_update<<<grid_for(b.ivol(), 256), 256, 0, stream>>>(
+        s, u1, ucs, rhs, rcs, b, dt, mode);
+}
+
+void launch_ccz4_probe(const double *s, const BoxDev &b, const Options &o,
+                       int i, int j, int k, double *out, cudaStream_t stream)
+{
+    k_ccz4_probe<<<1, 1, 0, stream>>>(s, b, o, i, j, k, out);
 }
 
 #define GRHD_INSTANTIATE(T)                                                   \

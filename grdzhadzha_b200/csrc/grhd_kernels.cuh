@@ -55,6 +55,7 @@ struct DevStatus
 enum : int
 {
     kStateComps = 11,
+    kCcz4GrhdOffset = 25, // GRHD components after GRChombo's CCZ4 ones
     kD = 0,
     kS1 = 1,
     kTau = 4,
@@ -202,5 +203,28 @@ template <typename T> cudaError_t ensemble_occupancy(int *blocks_per_sm);
 // One persistent launch of `grid` blocks (all resident; cooperative).
 template <typename T>
 cudaError_t launch_ensemble(const EnsLaunch &a, int grid, cudaStream_t s);
+
+// The operator on CCZ4-stored geometry (grhd_kernels.cu): state of 36
+// components (25 CCZ4, then 11 GRHD), stride b.cs; the geometry cache holds
+// gLL[6] gUU[6] lapse shift[3] over the ghosted box.
+void launch_ccz4_fill(double *s, const BoxDev &b, bool conserved,
+                      cudaStream_t st);
+void launch_ccz4_cells(const double *s, const BoxDev &b, const Options &o,
+                       double *prim, double *gc, DevStatus *st,
+                       cudaStream_t stream);
+void launch_ccz4_rhs(const double *s, const BoxDev &b, const Options &o,
+                     const double *prim, const double *gc, double *rhs,
+                     int64_t rcs, const double inv[3], DevStatus *st,
+                     cudaStream_t stream);
+void launch_ccz4_recover(double *s, const BoxDev &b, const Options &o,
+                         DevStatus *st, cudaStream_t stream);
+void launch_ccz4_max_inv_dt(const double *s, const BoxDev &b,
+                            const Options &o, const double inv[3],
+                            DevStatus *st, cudaStream_t stream);
+void launch_ccz4_update(double *s, const double *u1, int64_t ucs,
+                        const double *rhs, int64_t rcs, const BoxDev &b,
+                        double dt, int mode, cudaStream_t stream);
+void launch_ccz4_probe(const double *s, const BoxDev &b, const Options &o,
+                       int i, int j, int k, double *out, cudaStream_t stream);
 
 } // namespace grhd

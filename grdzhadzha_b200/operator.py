@@ -107,6 +107,7 @@ class LevelBox:
     domain_hi: tuple | None = None
     state: torch.Tensor | None = field(default=None, repr=False)
     device: str = "cuda"
+    ncomp: int = 11  # 36 (CCZ4 + GRHD) for LevelDataFiniteVolumeOperator
 
     def __post_init__(self):
         if self.domain_lo is None:
@@ -116,7 +117,7 @@ class LevelBox:
         if self.state is None:
             g = self.ghost
             n = [self.hi[d] - self.lo[d] + 1 + 2 * g for d in range(3)]
-            self.state = torch.zeros((11, n[2], n[1], n[0]),
+            self.state = torch.zeros((self.ncomp, n[2], n[1], n[0]),
                                      dtype=torch.float64, device=self.device)
 
     @classmethod
@@ -558,3 +559,111 @@ class TimeDependentFixedBGLevelDataFiniteVolumeOperator(_OperatorBase):
                        dt=None):
         return self._advance(self._lib.grhd_advance_ssprk2, state,
                              inverse_dx_U, time, dt)
+
+
+class LevelDataFiniteVolumeOperator:
+    """LevelDataFiniteVolumeOperator (FArrayBoxFiniteVolume.hpp:1215-1364):
+    the Valencia operator on a metric the grid holds in GRChombo's CCZ4
+    variables (grhd_ccz4_*).  States are LevelBoxes of
+    ncomp = GRHD_CCZ4_NUM_VARS components (25 CCZ4, then 11 GRHD); FP64."""
+
+    NUM_VARS = 36
+    GRHD_OFFSET = 25
+
+    def __init__(self, eos, atmosphere=None, limiter_theta=1.5,
+                 use_reconstruction=True, recovery_options=None,
+                 use_static_metric_sources=True):
+        self._lib = L.load()
+        p = L.Params()
+        self._lib.grhd_default_params(C.byref(p))
+        p.adiabatic_index = eos.adiabatic_index
+        p.dx = 1.0  # unused: the spacing comes with inverse_dx_U
+        a = atmosphere or AtmosphereOptions()
+        p.rho_floor, p.pressure_floor = a.rho_floor, a.pressure_floor
+        p.max_velocity_squared = a.max_velocity_squared
+        p.metric_source_atmosphere_factor = a.metric_source_atmosphere_factor
+        r = recovery_options or RecoveryOptions()
+        p.recovery_max_iterations = r.max_iterations
+        p.recovery_tolerance = r.tolerance
+        p.recovery_pressure_floor = r.pressure_floor
+        p.recovery_max_velocity_squared = r.max_velocity_squared
+        p.limiter_theta = limiter_theta
+        p.use_reconstruction = int(use_reconstruction)
+        p.use_static_metric_sources = int(use_static_metric_sources)
+        p.use_metric_volume_time_sources = 0
+        self.params = p
+        self.eos = eos
+        ctx = C.c_void_p()
+        L.check(self._lib, None, self._lib.grhd_create(C.byref(p),
+                                                       C.byref(ctx)))
+        self._ctx = ctx
+
+    def __del__(self):
+        ctx = getattr(self, "_ctx", None)
+        if ctx:
+            self._lib.grhd_destroy(ctx)
+
+    def _check(self, status):
+        L.check(self._lib, self._ctx, status)
+
+    @staticmethod
+    def _inv(inverse_dx_U):
+        if inverse_dx_U is None:
+            raise ValueError("inverse_dx_U is required")
+        return (C.c_double * 3)(*inverse_dx_U)
+
+    def _state(self, state: LevelBox):
+        if state.state.shape[0] != self.NUM_VARS:
+            raise ValueError(f"expected a {self.NUM_VARS}-component state")
+        return _ptr(state.state)
+
+    def compute_rhs(self, rhs, state: LevelBox, domain=None,
+                    inverse_dx_U=None):
+        b = state.c_box()
+        self._check(self._lib.grhd_ccz4_compute_rhs(
+            self._ctx, _ptr(rhs), rhs[0].numel(), self._state(state),
+            state.comp_stride(), C.byref(b), self._inv(inverse_dx_U),
+            _stream()))
+
+    def recover_primitives(self, state: LevelBox):
+        d = L.Diagnostics()
+        b = state.c_box()
+        self._check(self._lib.grhd_ccz4_recover_primitives(
+            self._ctx, self._state(state), state.comp_stride(), C.byref(b),
+            C.byref(d), _stream()))
+        return d
+
+    def update_conserved(self, state: LevelBox, rhs, dt,
+                         recover_primitives_after_update=True):
+        d = L.Diagnostics()
+        b = state.c_box()
+        self._check(self._lib.grhd_ccz4_update_conserved(
+            self._ctx, self._state(state), state.comp_stride(), _ptr(rhs),
+            rhs[0].numel(), C.byref(b), dt,
+            int(recover_primitives_after_update), C.byref(d), _stream()))
+        return d
+
+    def compute_max_inverse_dt(self, state: LevelBox, domain_box=None,
+                               inverse_dx_U=None):
+        out = C.c_double()
+        b = state.c_box()
+        self._check(self._lib.grhd_ccz4_compute_max_inverse_dt(
+            self._ctx, self._state(state), state.comp_stride(), C.byref(b),
+            self._inv(inverse_dx_U), C.byref(out), _stream()))
+        return out.value
+
+    def compute_stable_dt(self, state: LevelBox, domain_box=None,
+                          inverse_dx_U=None, cfl=None):
+        if cfl is None or not cfl > 0.0:
+            raise L.InvalidArgument(L.GRHD_ERR_INVALID_ARG, None)
+        m = self.compute_max_inverse_dt(state, domain_box, inverse_dx_U)
+        return cfl / max(m, 1.0e-14)
+
+    def advance_ssprk2(self, state: LevelBox, domain=None, inverse_dx_U=None,
+                       dt=None):
+        d = L.Diagnostics()
+        b = state.c_box()
+        self._check(self._lib.grhd_ccz4_advance_ssprk2(
+            self._ctx, self._state(state), state.comp_stride(), C.byref(b),
+            self._inv(inverse_dx_U), dt, C.byref(d), _stream()))
+        return d

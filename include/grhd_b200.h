@@ -428,6 +428,53 @@ int grhd_level_exchange(const grhd_box *boxes, double *const *states,
                         const int64_t *state_comp_strides, int count,
                         char *err, int err_cap, void *stream);
 
+/* ---- The operator on CCZ4-stored geometry ----
+ * LevelDataFiniteVolumeOperator (Source/Matter/GRHD/FArrayBoxFiniteVolume.hpp:
+ * 1215-1364): the same Valencia operator for a metric that the grid holds
+ * (dynamical-spacetime coupling).  The state has GRHD_CCZ4_NUM_VARS
+ * components of state_comp_stride doubles each: GRChombo's 25 CCZ4
+ * variables (chi, h11 h12 h13 h22 h23 h33, K, A11 A12 A13 A22 A23 A33,
+ * Theta, Gamma1..3, lapse, shift1..3, B1..3), then the 11 GRHD components
+ * in the order of the fixed-background state (Tests/GRHDFixedBGTest/
+ * UserVariables.hpp:24-40).  Geometry per cell: gamma = h / chi,
+ * gamma^-1 = chi h^-1, K_ij = A_ij / chi + gamma_ij K / 3, lapse, shift
+ * (load_ccz4_geometry, :168-192); the sources take their metric
+ * derivatives as finite differences of it (:219-427).  FP64 whatever the
+ * context's precision; the context's background, dx, centre, excision and
+ * accretion settings do not apply.  Physical ghosts copy the conserved
+ * variables and chi, h, lapse, shift of their source cell (:430-519). */
+#define GRHD_CCZ4_NUM_VARS 36
+#define GRHD_CCZ4_GRHD_OFFSET 25
+
+/* compute_rhs (:1232-1240): rhs (5 comps over the interior) = flux
+ * divergence + sources. */
+int grhd_ccz4_compute_rhs(grhd_ctx *ctx, double *rhs, int64_t rhs_comp_stride,
+                          double *state, int64_t state_comp_stride,
+                          const grhd_box *box, const double inverse_dx[3],
+                          void *stream);
+/* recover_primitives (:1272-1285). */
+int grhd_ccz4_recover_primitives(grhd_ctx *ctx, double *state,
+                                 int64_t state_comp_stride,
+                                 const grhd_box *box, grhd_diagnostics *diag,
+                                 void *stream);
+/* update_conserved (:1288-1299). */
+int grhd_ccz4_update_conserved(grhd_ctx *ctx, double *state,
+                               int64_t state_comp_stride, const double *rhs,
+                               int64_t rhs_comp_stride, const grhd_box *box,
+                               double dt, int recover, grhd_diagnostics *diag,
+                               void *stream);
+/* compute_max_inverse_dt (:1301-1307). */
+int grhd_ccz4_compute_max_inverse_dt(grhd_ctx *ctx, const double *state,
+                                     int64_t state_comp_stride,
+                                     const grhd_box *box,
+                                     const double inverse_dx[3], double *out,
+                                     void *stream);
+/* advance_ssprk2 (:1323-1348); the box must be the whole domain. */
+int grhd_ccz4_advance_ssprk2(grhd_ctx *ctx, double *state,
+                             int64_t state_comp_stride, const grhd_box *box,
+                             const double inverse_dx[3], double dt,
+                             grhd_diagnostics *diag, void *stream);
+
 /* The halo message of a level split over ranks (LevelData::exchange()
  * across MPI ranks in the reference): the 11 components of the cells
  * [lo, hi] (inside the ghosted box) into a packed device buffer laid out

@@ -2716,3 +2716,409 @@ void orc_kitp_viscous_rhs(const orc_params *p, const orc_kitp_config *k,
             }
 }
 
+
+/* ------------------------------------------------------------------------ */
+/* The operator on CCZ4-stored geometry (LevelDataFiniteVolumeOperator,      */
+/* Source/Matter/GRHD/FArrayBoxFiniteVolume.hpp:136-192, 219-542, 681-1364). */
+/* The state holds GRChombo's 25 CCZ4 variables, then the 11 GRHD ones       */
+/* (Tests/GRHDFixedBGTest/UserVariables.hpp:24-40); the geometry is read      */
+/* from chi, h_ij, A_ij, K, lapse and shift, and the metric derivatives of    */
+/* the sources are finite differences of it.                                 */
+/* ------------------------------------------------------------------------ */
+
+enum
+{
+    CZ_CHI = 0,
+    CZ_H = 1,      /* h11 h12 h13 h22 h23 h33 */
+    CZ_K = 7,
+    CZ_A = 8,      /* A11 A12 A13 A22 A23 A33 */
+    CZ_LAPSE = 18,
+    CZ_SHIFT = 19, /* shift1..3 */
+    CZ_GRHD = 25
+};
+
+static const int CZ_SYM[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+
+/* load_ccz4_geometry, :168-192 */
+static void ccz4_geometry(const orc_box *b, const double *s, int64_t idx,
+                          Geom *g)
+{
+    const int64_t cs = b->comp_stride;
+    const double chi = s[CZ_CHI * cs + idx];
+    double h[3][3], A[3][3], hUU[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+        {
+            h[i][j] = s[(CZ_H + CZ_SYM[i][j]) * cs + idx];
+            A[i][j] = s[(CZ_A + CZ_SYM[i][j]) * cs + idx];
+        }
+    inverse_sym(h, hUU);
+    const double trK = s[CZ_K * cs + idx];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+        {
+            g->gLL[i][j] = h[i][j] / chi;
+            g->gUU[i][j] = chi * hUU[i][j];
+            g->K[i][j] = A[i][j] / chi + g->gLL[i][j] * trK / 3.0;
+        }
+    g->lapse = s[CZ_LAPSE * cs + idx];
+    for (int i = 0; i < 3; ++i)
+        g->shift[i] = s[(CZ_SHIFT + i) * cs + idx];
+}
+
+/* Outflow source of a physical ghost (interior_box ends), or -1. */
+static int64_t ccz4_outflow_source(const orc_box *b, int i, int j, int k)
+{
+    const int iv[3] = {i, j, k};
+    int src[3] = {i, j, k};
+    int ghost = 0;
+    for (int d = 0; d < 3; ++d)
+    {
+        if (iv[d] < b->dlo[d])
+        {
+            ghost = 1;
+            src[d] = b->lo[d];
+        }
+        else if (iv[d] > b->dhi[d])
+        {
+            ghost = 1;
+            src[d] = b->hi[d];
+        }
+    }
+    return ghost ? fab_index(b, src[0], src[1], src[2]) : -1;
+}
+
+/* fill_conserved_outflow_boundaries (:484-519) and
+ * fill_ccz4_geometry_outflow_boundaries (:430-473): the physical ghosts
+ * copy the five conserved variables and chi, h_ij, lapse, shift of their
+ * source cell (the other CCZ4 variables and the primitives stay). */
+static void ccz4_fill_outflow(const orc_box *b, double *s, int conserved)
+{
+    const int64_t cs = b->comp_stride;
+    static const int geo[11] = {CZ_CHI, 1, 2, 3, 4, 5, 6, CZ_LAPSE,
+                                CZ_SHIFT, CZ_SHIFT + 1, CZ_SHIFT + 2};
+    for (int k = b->glo[2]; k <= b->ghi[2]; ++k)
+        for (int j = b->glo[1]; j <= b->ghi[1]; ++j)
+            for (int i = b->glo[0]; i <= b->ghi[0]; ++i)
+            {
+                const int64_t src = ccz4_outflow_source(b, i, j, k);
+                if (src < 0)
+                    continue;
+                const int64_t dst = fab_index(b, i, j, k);
+                if (conserved)
+                    for (int c = 0; c < 5; ++c)
+                        s[(CZ_GRHD + c) * cs + dst] =
+                            s[(CZ_GRHD + c) * cs + src];
+                for (int q = 0; q < 11; ++q)
+                    s[geo[q] * cs + dst] = s[geo[q] * cs + src];
+            }
+}
+
+static Cons ccz4_cons(const orc_box *b, const double *s, int64_t idx)
+{
+    return load_cons(b, s + CZ_GRHD * b->comp_stride, idx);
+}
+
+static Prim ccz4_prim(const orc_box *b, const double *s, int64_t idx)
+{
+    return load_prim(b, s + CZ_GRHD * b->comp_stride, idx);
+}
+
+/* compute_leveldata_flux_rhs_from_ccz4_geometry (:1047-1090) on one box:
+ * per direction the outflow fills, the ghosted-box recovery
+ * (recover_primitives_from_ccz4_geometry, :681-702), the MC slopes and the
+ * interior face pairs (:784-833, every face twice), summed into rhs; then
+ * the geometry fill and add_static_metric_sources_to_conserved_rhs
+ * (:367-427) with the one-sided stencils of
+ * make_metric_source_derivative_stencil (:283-322). */
+int orc_ccz4_compute_rhs(const orc_params *p, const orc_box *b, double *s,
+                         double *rhs, int64_t rcs, const double inv_dx[3],
+                         orc_error *err)
+{
+    if (err)
+        memset(err, 0, sizeof(*err));
+    if (!check_box(b))
+        return ORC_ERR_INVALID_ARG;
+    const int gnx = b->ghi[0] - b->glo[0] + 1, gny = b->ghi[1] - b->glo[1] + 1,
+              gnz = b->ghi[2] - b->glo[2] + 1;
+    const int64_t gvol = (int64_t)gnx * gny * gnz;
+    const int nx = b->hi[0] - b->lo[0] + 1, ny = b->hi[1] - b->lo[1] + 1;
+#define CZ_RIDX(i, j, k)                                                      \
+    ((int64_t)((i)-b->lo[0]) +                                                \
+     (int64_t)nx * ((int64_t)((j)-b->lo[1]) + (int64_t)ny * ((k)-b->lo[2])))
+    for (int k = b->lo[2]; k <= b->hi[2]; ++k)
+        for (int j = b->lo[1]; j <= b->hi[1]; ++j)
+            for (int i = b->lo[0]; i <= b->hi[0]; ++i)
+                for (int c = 0; c < 5; ++c)
+                    rhs[c * rcs + CZ_RIDX(i, j, k)] = 0.0;
+    Prim *prims = (Prim *)calloc(gvol, sizeof(Prim));
+    Geom *geo = (Geom *)calloc(gvol, sizeof(Geom));
+    int status = ORC_OK;
+    /* the fills and the recovery give the same values in every direction */
+    ccz4_fill_outflow(b, s, 1);
+    for (int k = b->glo[2]; k <= b->ghi[2] && status == ORC_OK; ++k)
+        for (int j = b->glo[1]; j <= b->ghi[1] && status == ORC_OK; ++j)
+            for (int i = b->glo[0]; i <= b->ghi[0]; ++i)
+            {
+                const int64_t idx = fab_index(b, i, j, k);
+                ccz4_geometry(b, s, idx, &geo[idx]);
+                const Cons c = ccz4_cons(b, s, idx);
+                int it;
+                double res;
+                if (!con2prim(p, &c, geo[idx].gUU, &prims[idx], &it, &res))
+                {
+                    set_error(err, ORC_ERR_RECOVERY,
+                              ORC_WHERE_GHOSTED_RECOVERY, i, j, k, res);
+                    status = ORC_ERR_RECOVERY;
+                    break;
+                }
+            }
+    for (int dir = 0; dir < 3 && status == ORC_OK; ++dir)
+    {
+        const int off[3] = {dir == 0, dir == 1, dir == 2};
+        const int64_t so = fab_index(b, b->lo[0] + off[0], b->lo[1] + off[1],
+                                     b->lo[2] + off[2]) -
+                           fab_index(b, b->lo[0], b->lo[1], b->lo[2]);
+        for (int k = b->lo[2]; k <= b->hi[2]; ++k)
+            for (int j = b->lo[1]; j <= b->hi[1]; ++j)
+                for (int i = b->lo[0]; i <= b->hi[0]; ++i)
+                {
+                    const int64_t c0 = fab_index(b, i, j, k);
+                    Flux f[2];
+                    for (int side = 0; side < 2; ++side)
+                    {
+                        /* face between L = c0 - so + side*so and L + so */
+                        const int64_t L = c0 - so + side * so, R = L + so;
+                        const Prim sl = prim_slope(&prims[L - so], &prims[L],
+                                                   &prims[R], p->limiter_theta);
+                        const Prim sr = prim_slope(&prims[L], &prims[R],
+                                                   &prims[R + so],
+                                                   p->limiter_theta);
+                        Geom g;
+                        average_geometry(&geo[L], &geo[R], &g);
+                        f[side] = muscl_hlle(p, &prims[L], &prims[R], &sl,
+                                             &sr, &g, dir);
+                    }
+                    const int64_t r = CZ_RIDX(i, j, k);
+                    const double idx_ = inv_dx[dir];
+                    rhs[0 * rcs + r] += -idx_ * (f[1].D - f[0].D);
+                    rhs[4 * rcs + r] += -idx_ * (f[1].tau - f[0].tau);
+                    for (int m = 0; m < 3; ++m)
+                        rhs[(1 + m) * rcs + r] += -idx_ * (f[1].S[m] - f[0].S[m]);
+                }
+    }
+    if (status == ORC_OK && p->use_static_metric_sources)
+    {
+        ccz4_fill_outflow(b, s, 0);
+        for (int k = b->lo[2]; k <= b->hi[2] && status == ORC_OK; ++k)
+            for (int j = b->lo[1]; j <= b->hi[1] && status == ORC_OK; ++j)
+                for (int i = b->lo[0]; i <= b->hi[0]; ++i)
+                {
+                    const int64_t idx = fab_index(b, i, j, k);
+                    Geom g;
+                    ccz4_geometry(b, s, idx, &g);
+                    const Cons c = ccz4_cons(b, s, idx);
+                    Prim pr;
+                    int it;
+                    double res;
+                    if (!con2prim(p, &c, g.gUU, &pr, &it, &res))
+                    {
+                        set_error(err, ORC_ERR_RECOVERY,
+                                  ORC_WHERE_METRIC_SOURCES, i, j, k, res);
+                        status = ORC_ERR_RECOVERY;
+                        break;
+                    }
+                    enforce_floors(p, &pr, g.gLL);
+                    if (is_atmosphere(p, &pr,
+                                      p->atmo_metric_source_atmosphere_factor))
+                        continue;
+                    Derivs dv;
+                    memset(&dv, 0, sizeof(dv));
+                    for (int dir = 0; dir < 3; ++dir)
+                    {
+                        const int off[3] = {dir == 0, dir == 1, dir == 2};
+                        const int64_t lo_i = fab_index(b, i - off[0], j - off[1],
+                                                       k - off[2]);
+                        const int64_t hi_i = fab_index(b, i + off[0], j + off[1],
+                                                       k + off[2]);
+                        const Prim pl = ccz4_prim(b, s, lo_i);
+                        const Prim pu = ccz4_prim(b, s, hi_i);
+                        const double f = p->atmo_metric_source_atmosphere_factor;
+                        const int la = !is_atmosphere(p, &pl, f);
+                        const int ua = !is_atmosphere(p, &pu, f);
+                        int64_t lo_c, up_c;
+                        double coef;
+                        if (la && ua)
+                        {
+                            lo_c = lo_i;
+                            up_c = hi_i;
+                            coef = 0.5 * inv_dx[dir];
+                        }
+                        else if (ua)
+                        {
+                            lo_c = idx;
+                            up_c = hi_i;
+                            coef = inv_dx[dir];
+                        }
+                        else if (la)
+                        {
+                            lo_c = lo_i;
+                            up_c = idx;
+                            coef = inv_dx[dir];
+                        }
+                        else
+                            continue;
+                        Geom gu, gl;
+                        ccz4_geometry(b, s, up_c, &gu);
+                        ccz4_geometry(b, s, lo_c, &gl);
+                        const int64_t cs = b->comp_stride;
+                        dv.dlapse[dir] = coef * (s[CZ_LAPSE * cs + up_c] -
+                                                 s[CZ_LAPSE * cs + lo_c]);
+                        dv.dlnsqrtg[dir] =
+                            coef * (log_sqrt_det(&gu) - log_sqrt_det(&gl));
+                        for (int a = 0; a < 3; ++a)
+                            for (int bb = 0; bb < 3; ++bb)
+                                dv.dgamma[dir][a][bb] =
+                                    coef * (gu.gLL[a][bb] - gl.gLL[a][bb]);
+                        for (int sd = 0; sd < 3; ++sd)
+                            dv.dshift[sd][dir] =
+                                coef * (s[(CZ_SHIFT + sd) * cs + up_c] -
+                                        s[(CZ_SHIFT + sd) * cs + lo_c]);
+                    }
+                    const Cons src = static_sources(p->gamma, &pr, &c, &g, &dv);
+                    const int64_t r = CZ_RIDX(i, j, k);
+                    rhs[0 * rcs + r] += src.D;
+                    rhs[4 * rcs + r] += src.tau;
+                    for (int m = 0; m < 3; ++m)
+                        rhs[(1 + m) * rcs + r] += src.S[m];
+                }
+    }
+#undef CZ_RIDX
+    free(prims);
+    free(geo);
+    return status;
+}
+
+/* recover_primitives_and_apply_atmosphere_from_ccz4_geometry (:713-761)
+ * over the interior. */
+void orc_ccz4_recover_primitives(const orc_params *p, const orc_box *b,
+                                 double *s, orc_diag *diag)
+{
+    memset(diag, 0, sizeof(*diag));
+    double *q = s + CZ_GRHD * b->comp_stride;
+    for (int k = b->lo[2]; k <= b->hi[2]; ++k)
+        for (int j = b->lo[1]; j <= b->hi[1]; ++j)
+            for (int i = b->lo[0]; i <= b->hi[0]; ++i)
+            {
+                ++diag->num_cells;
+                const int64_t idx = fab_index(b, i, j, k);
+                Geom g;
+                ccz4_geometry(b, s, idx, &g);
+                const Cons c = load_cons(b, q, idx);
+                Prim pr;
+                int it;
+                double res;
+                int reset = !con2prim(p, &c, g.gUU, &pr, &it, &res);
+                if (!reset)
+                {
+                    Prim fl = pr;
+                    enforce_floors(p, &fl, g.gLL);
+                    reset = prim_differs(&pr, &fl);
+                    if (reset)
+                        ++diag->num_floored_primitives;
+                    pr = fl;
+                }
+                else
+                {
+                    ++diag->num_failed_recoveries;
+                    pr = atmosphere_prim(p);
+                }
+                store_prim(b, q, idx, &pr);
+                if (reset)
+                {
+                    ++diag->num_conserved_resets;
+                    const Cons nc = p2c(p->gamma, &pr, g.gLL);
+                    store_cons(b, q, idx, &nc);
+                }
+            }
+}
+
+/* compute_max_inverse_dt_from_ccz4_geometry (:1139-1183). */
+int orc_ccz4_compute_max_inverse_dt(const orc_params *p, const orc_box *b,
+                                    const double *s, const double inv_dx[3],
+                                    double *out, orc_error *err)
+{
+    if (err)
+        memset(err, 0, sizeof(*err));
+    double m = 0.0;
+    for (int k = b->lo[2]; k <= b->hi[2]; ++k)
+        for (int j = b->lo[1]; j <= b->hi[1]; ++j)
+            for (int i = b->lo[0]; i <= b->hi[0]; ++i)
+            {
+                const int64_t idx = fab_index(b, i, j, k);
+                Geom g;
+                ccz4_geometry(b, s, idx, &g);
+                const Cons c = ccz4_cons(b, s, idx);
+                Prim pr;
+                int it;
+                double res;
+                if (!con2prim(p, &c, g.gUU, &pr, &it, &res))
+                {
+                    set_error(err, ORC_ERR_RECOVERY, ORC_WHERE_CFL, i, j, k,
+                              res);
+                    return ORC_ERR_RECOVERY;
+                }
+                enforce_floors(p, &pr, g.gLL);
+                if (is_atmosphere(p, &pr, 1.0 + 1.0e-12))
+                    continue;
+                double cell = 0.0;
+                for (int d = 0; d < 3; ++d)
+                {
+                    double lo, hi;
+                    char_speeds(p->gamma, &pr, g.gLL, g.gUU, d, g.lapse,
+                                g.shift, &lo, &hi);
+                    cell += dmax(fabs(lo), fabs(hi)) * inv_dx[d];
+                }
+                m = dmax(m, cell);
+            }
+    *out = m;
+    return ORC_OK;
+}
+
+/* The CCZ4 variables of a fixed background (the reference's fixed-BG vs
+ * CCZ4-geometry test fills them from the analytic metric,
+ * store_ccz4_background_vars, Tests/GRHDFixedBGTest/GRHDFixedBGTest.cpp:
+ * 97-134): chi = det(gamma)^(-1/3), h = gamma chi, A = K_ij chi - K h / 3,
+ * trace K, lapse, shift, over the
+ * ghosted box; the GRHD components are left as they are. */
+void orc_ccz4_fill_from_background(const orc_params *p, const orc_box *b,
+                                   double *s, double t)
+{
+    const int64_t cs = b->comp_stride;
+    for (int k = b->glo[2]; k <= b->ghi[2]; ++k)
+        for (int j = b->glo[1]; j <= b->ghi[1]; ++j)
+            for (int i = b->glo[0]; i <= b->ghi[0]; ++i)
+            {
+                const int64_t idx = fab_index(b, i, j, k);
+                double x, y, z;
+                cell_position(p, i, j, k, &x, &y, &z);
+                ADM v;
+                background_adm(p, t, x, y, z, &v);
+                const double chi = pow(det_sym(v.gamma), -1.0 / 3.0);
+                for (int q = 0; q < CZ_GRHD; ++q)
+                    s[q * cs + idx] = 0.0;
+                s[CZ_CHI * cs + idx] = chi;
+                for (int a = 0; a < 3; ++a)
+                    for (int c = a; c < 3; ++c)
+                    {
+                        const double h = v.gamma[a][c] * chi;
+                        s[(CZ_H + CZ_SYM[a][c]) * cs + idx] = h;
+                        s[(CZ_A + CZ_SYM[a][c]) * cs + idx] =
+                            v.K_tensor[a][c] * chi - v.K * h / 3.0;
+                    }
+                s[CZ_K * cs + idx] = v.K;
+                s[CZ_LAPSE * cs + idx] = v.lapse;
+                for (int a = 0; a < 3; ++a)
+                    s[(CZ_SHIFT + a) * cs + idx] = v.shift[a];
+            }
+}

@@ -266,6 +266,25 @@ void orc_kitp_sink_decay(const orc_params *p, const orc_kitp_config *k,
                          const orc_box *box, double *state, double t,
                          double dt);
 
+/* ---- the operator on CCZ4-stored geometry (LevelDataFiniteVolumeOperator,
+ * Source/Matter/GRHD/FArrayBoxFiniteVolume.hpp:681-1364) ----
+ * state: 36 components of comp_stride each, GRChombo's 25 CCZ4 variables
+ * (chi, h11 h12 h13 h22 h23 h33, K, A11..A33, Theta, Gamma1..3, lapse,
+ * shift1..3, B1..3) then the 11 GRHD ones. */
+#define ORC_CCZ4_NUM_VARS 36
+#define ORC_CCZ4_GRHD_OFFSET 25
+int orc_ccz4_compute_rhs(const orc_params *p, const orc_box *box,
+                         double *state, double *rhs, int64_t rhs_comp_stride,
+                         const double inv_dx[3], orc_error *err);
+void orc_ccz4_recover_primitives(const orc_params *p, const orc_box *box,
+                                 double *state, orc_diag *diag);
+int orc_ccz4_compute_max_inverse_dt(const orc_params *p, const orc_box *box,
+                                    const double *state,
+                                    const double inv_dx[3], double *out,
+                                    orc_error *err);
+void orc_ccz4_fill_from_background(const orc_params *p, const orc_box *box,
+                                   double *state, double t);
+
 #ifdef __cplusplus
 }
 #endif

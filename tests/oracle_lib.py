@@ -200,6 +200,14 @@ def lib():
         L.orc_kitp_sink_rhs.argtypes = [P, K, B, dp, dp, i64, C.c_double]
         L.orc_kitp_sink_decay.argtypes = [P, K, B, dp, C.c_double,
                                           C.c_double]
+        L.orc_ccz4_compute_rhs.argtypes = [P, B, dp, dp, i64, dp,
+                                           C.POINTER(Error)]
+        L.orc_ccz4_recover_primitives.argtypes = [P, B, dp, C.POINTER(Diag)]
+        L.orc_ccz4_recover_primitives.restype = None
+        L.orc_ccz4_compute_max_inverse_dt.argtypes = [P, B, dp, dp, dp,
+                                                      C.POINTER(Error)]
+        L.orc_ccz4_fill_from_background.argtypes = [P, B, dp, C.c_double]
+        L.orc_ccz4_fill_from_background.restype = None
         _lib = L
     return _lib
 
@@ -533,3 +541,51 @@ def run_disk_example(background: int, steps_cap: int | None = None):
             break
     final = x_split_diagnostics(p, box, state, time)
     return tp, init, final, steps
+
+
+# ---- the operator on CCZ4-stored geometry ----
+CCZ4_NUM_VARS = 36
+CCZ4_GRHD = 25
+
+
+def ccz4_state(p, box, grhd_state, time=0.0):
+    """36-component state: the CCZ4 variables of the fixed background (the
+    reference test's store_ccz4_background_vars), then the 11 GRHD
+    components of `grhd_state`."""
+    cs = box.comp_stride
+    s = np.zeros(CCZ4_NUM_VARS * cs, dtype=np.float64)
+    lib().orc_ccz4_fill_from_background(C.byref(p), C.byref(box), _dp(s),
+                                        time)
+    s[CCZ4_GRHD * cs:] = grhd_state
+    return s
+
+
+def ccz4_compute_rhs(p, box, state36):
+    n = interior_cells(box)
+    rhs = np.zeros(5 * n, dtype=np.float64)
+    inv = np.array([1.0 / p.dx] * 3)
+    err = Error()
+    st = lib().orc_ccz4_compute_rhs(C.byref(p), C.byref(box), _dp(state36),
+                                    _dp(rhs), n, _dp(inv), C.byref(err))
+    if st:
+        raise OracleError(st, err)
+    return rhs
+
+
+def ccz4_recover_primitives(p, box, state36) -> Diag:
+    d = Diag()
+    lib().orc_ccz4_recover_primitives(C.byref(p), C.byref(box), _dp(state36),
+                                      C.byref(d))
+    return d
+
+
+def ccz4_max_inverse_dt(p, box, state36):
+    out = C.c_double()
+    inv = np.array([1.0 / p.dx] * 3)
+    err = Error()
+    st = lib().orc_ccz4_compute_max_inverse_dt(
+        C.byref(p), C.byref(box), _dp(state36), _dp(inv), C.byref(out),
+        C.byref(err))
+    if st:
+        raise OracleError(st, err)
+    return out.value
