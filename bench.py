@@ -474,6 +474,122 @@ class CpuBaseline:
         return self.cells / el / 4.0
 
 
+# ------------------------------------------- widened rows (one GPU each)
+
+
+def _time(fn, reps=5, warmup=2):
+    """Average ms of fn() over reps calls, CUDA events on the current
+    stream, after warm-up."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def run_widened(hbm_peak):
+    """The library paths beyond the north-star step, each timed on its own
+    (inputs larger than L2 except where stated): the operator on CCZ4-
+    stored geometry, the multi-box level exchange, the split SSPRK2 of a
+    multi-box level, the KITP disk-driver source terms, the diagnostics
+    reduction and the halo pack of a slab face."""
+    import torch
+    import grdzhadzha_b200 as G
+    from grdzhadzha_b200 import workloads as W
+    from grdzhadzha_b200 import halo as H
+    out = {}
+    # operator on CCZ4-stored geometry, KS torus a = 0.9, 128^3 (660 MB)
+    n = 128
+    op, lv = W.kerr_schild_torus(n)
+    inv = [1.0 / op.dx] * 3
+    lv36 = op.ccz4_state(lv)
+    cop = G.LevelDataFiniteVolumeOperator(G.IdealGasEOS(op.eos.adiabatic_index))
+    rhs = lv36.new_rhs()
+    ms = _time(lambda: cop.compute_rhs(rhs, lv36, inverse_dx_U=inv))
+    frhs = lv.new_rhs()
+    ms_f = _time(lambda: op.compute_rhs(frhs, lv))
+    cells = lv.num_cells
+    # algorithmic bytes: the 36-component state read once, 5 written
+    alg = cells * (36 + 5) * 8
+    out["ccz4_rhs_128"] = {
+        "value": cells / (ms / 1e3), "unit": "cell-RHS/s", "ms": ms,
+        "fixed_background_rhs_ms": ms_f,
+        "hbm_frac": alg / (ms / 1e3) / 1e9 / hbm_peak,
+        "note": "FP64, every face twice, not tiled yet"}
+    del lv36, rhs, cop
+    # multi-box level: 256^3 cut into 8 z-slabs, exchange + split SSPRK2
+    n = 256
+    op, lv = W.kerr_schild_torus(n)
+    slabs = H.slab_boxes((0, 0, 0), (n - 1, n - 1, n - 1), 8)
+    boxes = []
+    for lo, hi in slabs:
+        b = G.LevelBox(lo=lo, hi=hi, ghost=2, domain_lo=(0, 0, 0),
+                       domain_hi=(n - 1,) * 3)
+        g = 2
+        b.state.copy_(lv.state[:, lo[2]:hi[2] + 2 * g + 1])
+        boxes.append(b)
+    stages = [G.LevelBox(lo=b.lo, hi=b.hi, ghost=2, domain_lo=b.domain_lo,
+                         domain_hi=b.domain_hi) for b in boxes]
+    moved = sum(H.region_cells(lo_, hi_)
+                for r in range(len(slabs))
+                for _, lo_, hi_ in H.halo_plan(slabs, r, (0, 0, 0),
+                                               (n - 1,) * 3)[1])
+    ms = _time(lambda: G.level_exchange(boxes), reps=10)
+    byts = moved * 11 * 8 * 2
+    out["level_exchange_256_8slabs"] = {
+        "value": byts / (ms / 1e3) / 1e9, "unit": "GB/s", "ms": ms,
+        "bytes": byts, "hbm_frac": byts / (ms / 1e3) / 1e9 / hbm_peak,
+        "note": "14 halo regions of 2 x 256^2 cells, read + written"}
+    dt = 0.5 * op.compute_stable_dt(lv, cfl=CFL)
+    ms_split = _time(lambda: op.advance_level_ssprk2(boxes, stages, dt),
+                     reps=3, warmup=1)
+    ms_fused = _time(lambda: op.advance_ssprk2(lv, dt=dt), reps=3, warmup=1)
+    out["ssprk2_256_8slabs"] = {
+        "value": lv.num_cells / (ms_split / 1e3), "unit": "cell-updates/s",
+        "ms": ms_split, "single_box_fused_ms": ms_fused}
+    # halo pack of one slab face (2 planes of 260^2 cells, 11 components)
+    face = (0, 0, slabs[1][0][2]), (n - 1, n - 1, slabs[1][0][2] + 1)
+    buf = torch.empty(11 * H.region_cells(*face), dtype=torch.float64,
+                      device="cuda")
+    reg = H.DeviceRegions()
+    ms = _time(lambda: reg.pack(boxes[1], face[0], face[1], buf), reps=20)
+    byts = buf.numel() * 8 * 2
+    out["halo_pack_face_256"] = {
+        "value": byts / (ms / 1e3) / 1e9, "unit": "GB/s", "ms": ms,
+        "bytes": byts}
+    # diagnostics reduction over the 256^3 torus
+    ms = _time(lambda: op.disk_diagnostics(lv), reps=5)
+    byts = lv.num_cells * 7 * 8
+    out["disk_diagnostics_256"] = {
+        "value": byts / (ms / 1e3) / 1e9, "unit": "GB/s", "ms": ms,
+        "hbm_frac": byts / (ms / 1e3) / 1e9 / hbm_peak,
+        "note": "7 state components read per cell; includes the host sum"}
+    del boxes, stages, lv, op
+    torch.cuda.empty_cache()
+    # KITP source terms on a binary-PN disk, 128^3
+    n = 128
+    op, lv = W.binary_pn_disk(n)
+    rhs = lv.new_rhs()
+    for name, fn in (("kitp_viscous_128",
+                      lambda: op.kitp_viscous_rhs(rhs, lv, time=0.0)),
+                     ("kitp_sink_rhs_128",
+                      lambda: op.kitp_sink_rhs(rhs, lv, time=0.0)),
+                     ("kitp_sink_decay_128",
+                      lambda: op.kitp_sink_decay(lv, 0.0, 1e-6))):
+        ms = _time(fn, reps=5)
+        out[name] = {"value": lv.num_cells / (ms / 1e3),
+                     "unit": "cells/s", "ms": ms}
+    torch.cuda.empty_cache()
+    return out
+
+
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -586,6 +702,11 @@ def main():
         ens["mixed"]["speedup_vs_fp64_plain"] = (
             ens["mixed"]["value"] / res["value"])
         variants["batched_ensemble"] = ens
+        try:
+            variants["widened"] = run_widened(hbm_peak)
+        except Exception as e:  # a failing extra leg keeps the bench line
+            variants["widened"] = {"error": repr(e)}
+        torch.cuda.empty_cache()
         if not args.no_adjoint:
             variants["adjoint"] = run_adjoint(
                 args.adjoint_n, args.adjoint_steps, args.adjoint_every,

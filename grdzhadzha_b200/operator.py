@@ -352,6 +352,55 @@ class _OperatorBase:
         for b, sb in zip(boxes, stage_boxes):
             self.ssprk2_stage(2, b, sb, dt, inverse_dx_U, time)
 
+    def ccz4_state(self, state: LevelBox, time=0.0) -> LevelBox:
+        """A 36-component LevelBox for LevelDataFiniteVolumeOperator: the
+        CCZ4 variables of this operator's analytic background over the
+        ghosted box (as the reference's store_ccz4_background_vars,
+        Tests/GRHDFixedBGTest/GRHDFixedBGTest.cpp:97-134: chi =
+        det(gamma)^(-1/3), h = gamma chi, A = K_ij chi - K h / 3, trace K,
+        lapse, shift; the others zero), then the 11 GRHD components of
+        `state`.  The metric comes from grhd_eval_background."""
+        g = state.ghost
+        dev = state.state.device
+        idx = [torch.arange(state.lo[d] - g, state.hi[d] + g + 1,
+                            dtype=torch.float64, device=dev)
+               for d in range(3)]
+        z, y, x = torch.meshgrid(idx[2], idx[1], idx[0], indexing="ij")
+        c = self.params.center
+        xyz = torch.stack([(x + 0.5) * self.dx - c[0],
+                           (y + 0.5) * self.dx - c[1],
+                           (z + 0.5) * self.dx - c[2]], dim=-1).reshape(-1, 3)
+        xyz = xyz.contiguous()
+        out = torch.empty((xyz.shape[0], 64), dtype=torch.float64, device=dev)
+        self._check(self._lib.grhd_eval_background(
+            self._ctx, xyz.shape[0], _ptr(xyz), time, _ptr(out), _stream()))
+        gm = out[:, 0:9].reshape(-1, 3, 3)
+        Kt = out[:, 9:18].reshape(-1, 3, 3)
+        trK, lapse, shift = out[:, 18], out[:, 19], out[:, 20:23]
+        det = (gm[:, 0, 0] * gm[:, 1, 1] * gm[:, 2, 2]
+               + 2 * gm[:, 0, 1] * gm[:, 0, 2] * gm[:, 1, 2]
+               - gm[:, 0, 0] * gm[:, 1, 2] * gm[:, 1, 2]
+               - gm[:, 1, 1] * gm[:, 0, 2] * gm[:, 0, 2]
+               - gm[:, 2, 2] * gm[:, 0, 1] * gm[:, 0, 1])
+        chi = torch.pow(det, -1.0 / 3.0)
+        shape = state.state.shape[1:]
+        lv = LevelBox(lo=state.lo, hi=state.hi, ghost=g,
+                      domain_lo=state.domain_lo, domain_hi=state.domain_hi,
+                      device=str(dev), ncomp=36)
+        v = lv.state
+        v[0] = chi.reshape(shape)
+        pairs = [(0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2)]
+        for q, (a, b) in enumerate(pairs):
+            h = gm[:, a, b] * chi
+            v[1 + q] = h.reshape(shape)
+            v[8 + q] = (Kt[:, a, b] * chi - trK * h / 3.0).reshape(shape)
+        v[7] = trK.reshape(shape)
+        v[18] = lapse.reshape(shape)
+        for d in range(3):
+            v[19 + d] = shift[:, d].reshape(shape)
+        v[25:] = state.state
+        return lv
+
     # ---- initial data (FixedBGTorus.hpp, Michel test) ----
 
     def fill_torus(self, state: LevelBox, inner_radius, pressure_max_radius,

@@ -10,7 +10,8 @@ from __future__ import annotations
 
 import numpy as np
 
-from .operator import (AtmosphereOptions, IdealGasEOS, KerrSchild, LevelBox,
+from .operator import (AtmosphereOptions, CircularBinaryPN, IdealGasEOS,
+                       KerrSchild, LevelBox,
                        RecoveryOptions,
                        TimeDependentFixedBGLevelDataFiniteVolumeOperator)
 
@@ -46,6 +47,32 @@ def kerr_schild_torus(n, spin=0.9, half_width=40.0, gamma=5.0 / 3.0,
                   max_velocity_squared=0.8)
     if perturbation:
         op.perturb_density(lv, perturbation, seed)
+    op.recover_primitives(lv)
+    return op, lv
+
+
+def binary_pn_disk(n, half_width=40.0, gamma=5.0 / 3.0, inner_radius=14.0,
+                   pressure_max_radius=18.0, rho_peak=2e-5, separation=8.0,
+                   softening_radius=1.0, precision="fp64", device="cuda"):
+    """Circumbinary torus around the circular PN binary (masses 0.5 + 0.5,
+    separation 8, softening 1; the binary disk drivers' setting) on an n^3
+    grid over [-half_width, half_width]^3: atmosphere 1e-10 / 1e-12 / v^2
+    cap 0.8, MUSCL-MC (theta 1.4) + HLLE, volume-time source on.  Returns
+    (operator, level)."""
+    nn = (n, n, n) if isinstance(n, int) else tuple(n)
+    dx = 2.0 * half_width / nn[0]
+    c = tuple(0.5 * nn[d] * dx for d in range(3))
+    op = TimeDependentFixedBGLevelDataFiniteVolumeOperator(
+        IdealGasEOS(gamma),
+        CircularBinaryPN(mass_1=0.5, mass_2=0.5, separation=separation,
+                         softening_radius=softening_radius, dx=dx),
+        dx, c, AtmosphereOptions(1e-10, 1e-12, 0.8), 1.4, True,
+        RecoveryOptions(80, 1e-12, 1e-12, 0.8), True, True, 1e-3, 0.0, 0.0,
+        precision)
+    lv = LevelBox.cube(nn, device=device)
+    op.fill_torus(lv, inner_radius=inner_radius,
+                  pressure_max_radius=pressure_max_radius, rho_peak=rho_peak,
+                  max_velocity_squared=0.8)
     op.recover_primitives(lv)
     return op, lv
 

@@ -185,3 +185,17 @@ def test_ccz4_rejects_an_eleven_component_state():
     lv = G.LevelBox(lo=(0, 0, 0), hi=(3, 3, 3))
     with pytest.raises(ValueError):
         op.compute_rhs(lv.new_rhs(), lv, inverse_dx_U=[4.0] * 3)
+
+
+def test_ccz4_state_from_background_matches_oracle():
+    """The library's device-side CCZ4 fill (via grhd_eval_background)
+    against the oracle's restatement of the reference test's
+    store_ccz4_background_vars: within 1e-14 of each variable's scale."""
+    p, box, s = _case("ksdisk")
+    op = cases.gpu_operator(p)
+    lv = op.ccz4_state(cases.gpu_level(box, s))
+    got = lv.state.cpu().numpy().reshape(O.CCZ4_NUM_VARS, -1)
+    want = O.ccz4_state(p, box, s).reshape(O.CCZ4_NUM_VARS, -1)
+    scale = np.maximum(np.abs(want).max(axis=1), 1e-300)
+    err = np.abs(got - want).max(axis=1) / scale
+    assert np.all(err <= 1e-14), err
