@@ -1681,7 +1681,6 @@ template <typename T> size_t faces_smem()
 
 constexpr int kCzChi = 0, kCzH = 1, kCzK = 7, kCzA = 8, kCzLapse = 18,
               kCzShift = 19;
-constexpr int kCzGeoFields = 16; // gLL[6] gUU[6] lapse shift[3]
 
 // load_ccz4_geometry (:168-192): gamma = h / chi, gamma^-1 = chi h^-1 (the
 // symmetric cofactor inverse of GRChombo's TensorAlgebra), K_ij = A_ij /
@@ -1723,6 +1722,7 @@ __device__ __forceinline__ void ccz4_geo(const double *__restrict__ s,
         geo.shift[d] = s[(kCzShift + d) * cs + g];
 }
 
+// The geometry cache: gLL[6] gUU[6] lapse shift[3] per ghosted cell.
 __device__ __forceinline__ void geo_put(double *gc, int64_t n, int64_t g,
                                         const Geo &v)
 {
