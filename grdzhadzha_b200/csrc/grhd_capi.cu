@@ -785,10 +785,14 @@ void enqueue_ssprk2(grhd_ctx *ctx, double *state, const BoxDev &b,
 // combination is fused with the post-update recovery at the next RHS time
 // and with that RHS's per-cell work; the last stage optionally computes the
 // next CFL speed.  No host synchronisation.
+// prepped_in: the primitive cache and sources already hold the first
+// RHS's per-cell pass (done by the previous step's last stage); prep_out:
+// the last stage does that pass for the next step.
 template <typename T>
 void enqueue_rk4(grhd_ctx *ctx, double *state, const BoxDev &b,
                  const double inverse_dx[3], double time, double dt,
-                 bool want_cfl, cudaStream_t s)
+                 bool want_cfl, cudaStream_t s, bool prepped_in = false,
+                 bool prep_out = false)
 {
     BoxDev sb = b;
     sb.cs = b.gvol();
@@ -803,7 +807,8 @@ void enqueue_rk4(grhd_ctx *ctx, double *state, const BoxDev &b,
     {
         const double w = (dt / 6.0) * ((stage == 1 || stage == 2) ? 2.0 : 1.0);
         if (stage == 0)
-            enqueue_rhs<T>(ctx, k, state, b, bgs[0], inverse_dx, s, false, w);
+            enqueue_rhs<T>(ctx, k, state, b, bgs[0], inverse_dx, s,
+                           prepped_in, w);
         else
             enqueue_rhs<T>(ctx, k, ctx->stage, sb, bgs[stage], inverse_dx, s,
                            true, w);
@@ -815,20 +820,23 @@ void enqueue_rk4(grhd_ctx *ctx, double *state, const BoxDev &b,
                             ctx->status, s);
         else
             launch_stage<T>(0, state, b.cs, nullptr, 0, state, b.cs, k,
-                            ctx->acc, prim, nullptr, false, b, bgs[3],
-                            ctx->opt, stage, dt, want_cfl, inverse_dx,
-                            ctx->status, s);
+                            ctx->acc, prim, prep_out ? src : nullptr,
+                            prep_out ? 3 : 0, b, bgs[3], ctx->opt, stage, dt,
+                            want_cfl, inverse_dx, ctx->status, s);
     }
 }
 
 void enqueue_rk4_any(grhd_ctx *ctx, double *state, const BoxDev &b,
                      const double inverse_dx[3], double time, double dt,
-                     bool want_cfl, cudaStream_t s)
+                     bool want_cfl, cudaStream_t s, bool prepped_in = false,
+                     bool prep_out = false)
 {
     if (ctx->params.precision == GRHD_PRECISION_MIXED)
-        enqueue_rk4<float>(ctx, state, b, inverse_dx, time, dt, want_cfl, s);
+        enqueue_rk4<float>(ctx, state, b, inverse_dx, time, dt, want_cfl, s,
+                           prepped_in, prep_out);
     else
-        enqueue_rk4<double>(ctx, state, b, inverse_dx, time, dt, want_cfl, s);
+        enqueue_rk4<double>(ctx, state, b, inverse_dx, time, dt, want_cfl, s,
+                            prepped_in, prep_out);
 }
 
 // advance_ssprk2 (:563-589) cut at its two RHS evaluations, for a level
@@ -1194,6 +1202,74 @@ int grhd_advance_rk4_cfl(grhd_ctx *ctx, double *state, int64_t state_cs,
     *max_inverse_dt = bits_to_double(ctx->status_h->maxinv_bits);
     if (dt_used)
         *dt_used = dt;
+    return GRHD_OK;
+}
+
+int grhd_advance_rk4_cfl_steps(grhd_ctx *ctx, double *state,
+                               int64_t state_cs, const grhd_box *box,
+                               const double inverse_dx[3], double time,
+                               double cfl, double max_dt, int steps,
+                               double *max_inverse_dt, double *time_out,
+                               grhd_diagnostics *diag, void *stream)
+{
+    if (ctx && (!(cfl > 0.0) || !max_inverse_dt || steps < 0))
+    {
+        std::memset(&ctx->last_error, 0, sizeof(ctx->last_error));
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "GRHD CFL number must be positive");
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    BoxDev b;
+    int st = advance_checks(ctx, state, state_cs, box, inverse_dx, b, s);
+    if (st)
+        return st;
+    grhd_diagnostics total{};
+    double mi = *max_inverse_dt;
+    if (!(mi > 0.0) && steps > 0)
+    {
+        const Background bg0 = make_background(ctx->params, time);
+        {
+            Timed t_(ctx, GRHD_K_CFL, s);
+            launch_max_inv_dt(state, b, bg0, ctx->opt, inverse_dx,
+                              ctx->status,
+                              ctx->params.precision == GRHD_PRECISION_MIXED,
+                              s);
+        }
+        if ((st = finish_status(ctx, b, state, bg0, s)))
+            return st;
+        mi = bits_to_double(ctx->status_h->maxinv_bits);
+        if ((st = reset_status(ctx, s)))
+            return st;
+    }
+    for (int n = 0; n < steps; ++n)
+    {
+        double dt = cfl / std::fmax(mi, 1.0e-14);
+        if (max_dt > 0.0)
+            dt = std::fmin(dt, max_dt);
+        enqueue_rk4_any(ctx, state, b, inverse_dx, time, dt, true, s, n > 0,
+                        n + 1 < steps);
+        st = finish_status(ctx, b, state, make_background(ctx->params, time),
+                           s);
+        grhd_diagnostics d{};
+        read_diag(ctx, &d);
+        total.num_cells += d.num_cells;
+        total.num_failed_recoveries += d.num_failed_recoveries;
+        total.num_floored_primitives += d.num_floored_primitives;
+        total.num_conserved_resets += d.num_conserved_resets;
+        if (st)
+            break;
+        mi = bits_to_double(ctx->status_h->maxinv_bits);
+        time += dt;
+        if (n + 1 < steps && (st = reset_status(ctx, s)))
+            break;
+    }
+    if (diag)
+        *diag = total;
+    if (st)
+        return st;
+    *max_inverse_dt = mi;
+    if (time_out)
+        *time_out = time;
     return GRHD_OK;
 }
 

@@ -1170,14 +1170,17 @@ __global__ void __launch_bounds__(256, kMinBlocks<T>)
     const int64_t n = b.ivol();
     const int64_t n_pad = (n + blockDim.x - 1) / blockDim.x * blockDim.x;
     const double inv[3] = {i0, i1, i2};
-    const bool prep = prep_flag != 0 && prim != nullptr;
+    // prep_flag bit 0: the next RHS's per-cell pass; bit 1: the output
+    // keeps its primitives even so (the last RK4 stage of a multi-step call)
+    const bool prep = (prep_flag & 1) && prim != nullptr;
+    const bool store_p = !prep || (prep_flag & 2);
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n_pad;
          t += (int64_t)gridDim.x * blockDim.x)
     {
         double cell_inv = 0.0;
         if (t < n)
             stage_item<MODE, T>(un, ucs, us, tcs, out, ocs, kv, acc, prim, src,
-                                b, bg, o, stage, dt, prep, !prep, cfl != 0,
+                                b, bg, o, stage, dt, prep, store_p, cfl != 0,
                                 inv, st, t, cnt, cell_inv);
         flush_counts(st, cnt);
         cnt[0] = cnt[1] = cnt[2] = cnt[3] = 0;
@@ -2210,7 +2213,7 @@ void launch_recover(double *state, const BoxDev &b, const Background &bg,
 template <typename T>
 void launch_stage(int mode, const double *un, int64_t ucs, const double *us,
                   int64_t tcs, double *out, int64_t ocs, const T *k,
-                  double *acc, T *prim, T *src, bool prep, const BoxDev &b,
+                  double *acc, T *prim, T *src, int prep, const BoxDev &b,
                   const Background &bg, const Options &o, int stage,
                   double dt, bool cfl, const double inv_dx[3], DevStatus *st,
                   cudaStream_t s)
@@ -2218,7 +2221,7 @@ void launch_stage(int mode, const double *un, int64_t ucs, const double *us,
     const int grid = grid_for(b.ivol(), 256);
     const double i0 = inv_dx ? inv_dx[0] : 0.0, i1 = inv_dx ? inv_dx[1] : 0.0,
                  i2 = inv_dx ? inv_dx[2] : 0.0;
-    const int pf = prep ? 1 : 0, cf = cfl ? 1 : 0;
+    const int pf = prep, cf = cfl ? 1 : 0;
     if (mode == 0)
         k_stage<0, T><<<grid, 256, 0, s>>>(un, ucs, us, tcs, out, ocs, k, acc,
                                            prim, src, b, bg, o, stage, dt, pf,
@@ -2343,7 +2346,7 @@ void launch_ccz4_probe(const double *s, const BoxDev &b, const Options &o,
                                   cudaStream_t);                              \
     template void launch_stage<T>(int, const double *, int64_t,               \
                                   const double *, int64_t, double *, int64_t, \
-                                  const T *, double *, T *, T *, bool,        \
+                                  const T *, double *, T *, T *, int,         \
                                   const BoxDev &, const Background &,         \
                                   const Options &, int, double, bool,         \
                                   const double *, DevStatus *, cudaStream_t);

@@ -117,7 +117,7 @@ void launch_recover(double *state, const BoxDev &b, const Background &bg,
 template <typename T>
 void launch_stage(int mode, const double *un, int64_t ucs, const double *us,
                   int64_t tcs, double *out, int64_t ocs, const T *k,
-                  double *acc, T *prim, T *src, bool prep, const BoxDev &b,
+                  double *acc, T *prim, T *src, int prep, const BoxDev &b,
                   const Background &bg, const Options &o, int stage,
                   double dt, bool cfl, const double inv_dx[3], DevStatus *st,
                   cudaStream_t s);

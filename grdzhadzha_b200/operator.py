@@ -529,6 +529,24 @@ class _OperatorBase:
             C.byref(dt), C.byref(d), _stream()))
         return dt.value, mi.value, d
 
+    def advance_rk4_cfl_steps(self, state, cfl, steps, time=0.0, max_dt=0.0,
+                              max_inverse_dt=0.0, inverse_dx_U=None):
+        """New: `steps` advance_rk4_cfl steps in one call
+        (grhd_advance_rk4_cfl_steps); the per-cell pass of each step's
+        first RHS rides on the previous step's last stage.  Returns
+        (time reached, next max_inverse_dt, diagnostics of all steps)."""
+        if not cfl > 0.0:
+            raise L.InvalidArgument(L.GRHD_ERR_INVALID_ARG, None)
+        mi = C.c_double(max_inverse_dt)
+        tout = C.c_double(time)
+        d = L.Diagnostics()
+        b = state.c_box()
+        self._check(self._lib.grhd_advance_rk4_cfl_steps(
+            self._ctx, _ptr(state.state), state.comp_stride(), C.byref(b),
+            self._inv(inverse_dx_U), time, cfl, max_dt, int(steps),
+            C.byref(mi), C.byref(tout), C.byref(d), _stream()))
+        return tout.value, mi.value, d
+
 
 class FixedBGLevelDataFiniteVolumeOperator(_OperatorBase):
     """FixedBGFArrayBoxFiniteVolume.hpp:446-614 (static background)."""

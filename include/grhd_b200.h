@@ -256,6 +256,21 @@ int grhd_advance_rk4_cfl(grhd_ctx *ctx, double *state,
                          double *dt_used, grhd_diagnostics *diag,
                          void *stream);
 
+/* New: `steps` calls of grhd_advance_rk4_cfl in one (each step's dt from
+ * the CFL speed of its input state, capped by max_dt; *max_inverse_dt in
+ * and out as there), for a driver that advances several steps between
+ * looks at the state: the last stage of each step also does the per-cell
+ * pass (con2prim, sources) of the next step's first RHS, which a separate
+ * call has to redo.  time_out (may be NULL) receives the time reached;
+ * `diag` (may be NULL) the counts of every recovery of every step. */
+int grhd_advance_rk4_cfl_steps(grhd_ctx *ctx, double *state,
+                               int64_t state_comp_stride,
+                               const grhd_box *box,
+                               const double inverse_dx[3], double time,
+                               double cfl, double max_dt, int steps,
+                               double *max_inverse_dt, double *time_out,
+                               grhd_diagnostics *diag, void *stream);
+
 /* ---- pointwise kernels for verification ---- */
 
 /* ADM background vars at n points (xyz[3n], positions relative to the

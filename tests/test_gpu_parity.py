@@ -142,6 +142,39 @@ def test_rk4_cfl_steps_match_oracle(name, G):
     assert np.all(err <= 1e-11), err
 
 
+@pytest.mark.parametrize("name", ["torus_a09", "michel_c1", "pndisk",
+                                  "ksdisk"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_rk4_cfl_multi_step_call_matches_single_steps(name, precision, G):
+    """grhd_advance_rk4_cfl_steps (the next step's per-cell pass done in
+    the previous step's last stage) against the same number of
+    advance_rk4_cfl calls: FP64 bit for bit (the same con2prim of the same
+    state); mixed within 1e-6 of the state's scale (the separate call's
+    first con2prim starts from the stored pressure, the fused one reuses
+    the stage's converged solve: equal to the solver tolerance, then
+    rounded to FP32 in the primitive cache)."""
+    p, box, s, t = cases.CASES[name]()
+    a, b = cases.gpu_level(box, s), cases.gpu_level(box, s)
+    op = cases.gpu_operator(p, precision=precision)
+    mi, ta, cells = 0.0, t, 0
+    for _ in range(3):
+        dt, mi, d = op.advance_rk4_cfl(a, 0.25, time=ta, max_inverse_dt=mi)
+        ta += dt
+        cells += d.num_cells
+    op2 = cases.gpu_operator(p, precision=precision)
+    tb, mib, db = op2.advance_rk4_cfl_steps(b, 0.25, 3, time=t)
+    assert db.num_cells == cells
+    if precision == "fp64":
+        assert torch.equal(a.state, b.state)
+        assert tb == ta and mib == mi
+    else:
+        err = cases.rel_err(b.state.cpu().numpy().reshape(11, -1)[:5],
+                            a.state.cpu().numpy().reshape(11, -1)[:5])
+        print(f"{name} mixed multi-step vs single steps: {err}")
+        assert np.all(err <= 1e-6), err
+        assert abs(tb - ta) <= 1e-6 * abs(ta - t)
+
+
 def test_ks_disk_golden_on_gpu(G):
     """The Kerr-Schild disk example (40 SSPRK2 steps) on the GPU reproduces
     the reference's recorded disk mass (GRHD_PROGRESS.md:396-409)."""
