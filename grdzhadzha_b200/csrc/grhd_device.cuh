@@ -382,13 +382,15 @@ __device__ __forceinline__ void pn_metric(const Background &bg, T x, T y, T z,
     f->g = g;
 }
 
-template <bool FULL>
+// BGK: the background kind when known at compile time (0 Kerr-Schild,
+// 1 binary PN), -1 to read it from bg.kind.
+template <bool FULL, int BGK = -1>
 __device__ __forceinline__ void background_metric(const Background &bg,
                                                   double x, double y,
                                                   double z, Geo &g,
                                                   GeoFull *f)
 {
-    if (bg.kind == 1)
+    if (BGK == 1 || (BGK < 0 && bg.kind == 1))
         pn_metric<double, FULL>(bg, x, y, z, g, f);
     else
         ks_metric<double, FULL>(bg.M, bg.a, x, y, z, g, f);
@@ -444,14 +446,14 @@ __device__ __noinline__ void ks_metric_fp64_to_fp32(double M, double a,
 // radii of a Kerr-Schild hole where the metric (and so its determinant and
 // inverse) is evaluated in FP64 -- there r^2 = (rho^2 - a^2)/2 + ... and
 // 1 + 2H lose too many FP32 digits.
-template <bool FULL>
+template <bool FULL, int BGK = -1>
 __device__ __forceinline__ void background_metric_mixed(const Background &bg,
                                                         double x, double y,
                                                         double z,
                                                         GeoT<float> &g,
                                                         GeoFullT<float> *f)
 {
-    if (bg.kind == 1)
+    if (BGK == 1 || (BGK < 0 && bg.kind == 1))
         pn_metric<float, FULL>(bg, float(x), float(y), float(z), g, f);
     else if (x * x + y * y + z * z < 9.0 * bg.M * bg.M)
         ks_metric_fp64_to_fp32<FULL>(bg.M, bg.a, x, y, z, g, f);
@@ -460,43 +462,15 @@ __device__ __forceinline__ void background_metric_mixed(const Background &bg,
                                float(z), g, f);
 }
 
-template <typename T, bool FULL>
+template <typename T, bool FULL, int BGK = -1>
 __device__ __forceinline__ void metric_T(const Background &bg, double x,
                                          double y, double z, GeoT<T> &g,
-                                         GeoFullT<T> *f);
-
-template <>
-__device__ __forceinline__ void metric_T<double, false>(const Background &bg,
-                                                       double x, double y,
-                                                       double z, Geo &g,
-                                                       GeoFull *f)
+                                         GeoFullT<T> *f)
 {
-    background_metric<false>(bg, x, y, z, g, f);
-}
-template <>
-__device__ __forceinline__ void metric_T<double, true>(const Background &bg,
-                                                      double x, double y,
-                                                      double z, Geo &g,
-                                                      GeoFull *f)
-{
-    background_metric<true>(bg, x, y, z, g, f);
-}
-template <>
-__device__ __forceinline__ void metric_T<float, false>(const Background &bg,
-                                                      double x, double y,
-                                                      double z,
-                                                      GeoT<float> &g,
-                                                      GeoFullT<float> *f)
-{
-    background_metric_mixed<false>(bg, x, y, z, g, f);
-}
-template <>
-__device__ __forceinline__ void metric_T<float, true>(const Background &bg,
-                                                     double x, double y,
-                                                     double z, GeoT<float> &g,
-                                                     GeoFullT<float> *f)
-{
-    background_metric_mixed<true>(bg, x, y, z, g, f);
+    if constexpr (sizeof(T) == sizeof(double))
+        background_metric<FULL, BGK>(bg, x, y, z, g, f);
+    else
+        background_metric_mixed<FULL, BGK>(bg, x, y, z, g, f);
 }
 
 // Coordinates<double>: cell centre (i + 1/2) dx - centre, rounded as the

@@ -503,7 +503,7 @@ __device__ __forceinline__ PVT<T> load_pv_smem(const T *P, int cell)
 }
 
 // Geometry of the cross-shaped (x,y) neighbourhood of a tile at plane kk.
-template <typename T>
+template <typename T, int BGK = -1>
 __device__ __forceinline__ void tile_geometry(T *G, const Background &bg,
                                               const Options &o, int i0,
                                               int j0, int kk, int tid)
@@ -517,7 +517,7 @@ __device__ __forceinline__ void tile_geometry(T *G, const Background &bg,
         double x, y, z;
         cell_xyz(o, i0 - 1 + u, j0 - 1 + v, kk, x, y, z);
         GeoT<T> g;
-        metric_T<T, false>(bg, x, y, z, g, nullptr);
+        metric_T<T, false, BGK>(bg, x, y, z, g, nullptr);
         geo_store(G, n, idx, g);
     }
 }
@@ -575,7 +575,7 @@ __device__ __forceinline__ void block_partial(double v, double *scratch,
 // register window (each z face once); divergence + sources to the RHS.
 // One tile (bx, by, bz) of the face pass; 16x16 threads, `smem_raw` holds
 // faces_smem<T>() bytes; the tile's accretion sum goes to mdot_part[part].
-template <typename T, bool MDOT, bool CG = false>
+template <typename T, bool MDOT, bool CG = false, int BGK = -1>
 __device__ __forceinline__ void
 faces_tile(const T *__restrict__ prim, const T *__restrict__ src,
            T *__restrict__ rhs, const BoxDev &b, const Background &bg,
@@ -607,7 +607,7 @@ faces_tile(const T *__restrict__ prim, const T *__restrict__ src,
     PVT<T> w0, w1, w2, w3;
     ConsT<T> Flo = zero_cons<T>();
     double macc = 0.0;
-    tile_geometry(Gb, bg, o, i0, j0, k0, tid);
+    tile_geometry<T, BGK>(Gb, bg, o, i0, j0, k0, tid);
     __syncthreads();
     {
         w0 = load_pv_global<T, CG>(prim, b.pcs, b.gidx(ci_c, cj_c, k0 - 2));
@@ -619,7 +619,7 @@ faces_tile(const T *__restrict__ prim, const T *__restrict__ src,
             double x, y, z;
             cell_xyz(o, ci, cj, k0 - 1, x, y, z);
             GeoT<T> gl, gr, gf;
-            metric_T<T, false>(bg, x, y, z, gl, nullptr);
+            metric_T<T, false, BGK>(bg, x, y, z, gl, nullptr);
             geo_load(Gb, nG, (bb + 1) * kGW + (a + 1), gr);
             average_geo(gl, gr, gf);
             Flo = face_flux(o, w0, w1, w2, w3, gf, 2);
@@ -653,7 +653,7 @@ faces_tile(const T *__restrict__ prim, const T *__restrict__ src,
             for (int c = 0; c < 5; ++c)
                 P[c * nP + idx] = rdro<CG>(&prim[c * b.pcs + g]);
         }
-        tile_geometry(Gn, bg, o, i0, j0, k + 1, tid);
+        tile_geometry<T, BGK>(Gn, bg, o, i0, j0, k + 1, tid);
         __syncthreads();
 
         // x face between cells (i0+a-1, i0+a) in row j0+bb
@@ -748,7 +748,7 @@ faces_tile(const T *__restrict__ prim, const T *__restrict__ src,
                       tid, kTB * kTB, part);
 }
 
-template <typename T, bool MDOT>
+template <typename T, bool MDOT, int BGK>
 __global__ void __launch_bounds__(kTB *kTB, kMinBlocks<T>)
     k_faces(const T *__restrict__ prim, const T *__restrict__ src,
             T *__restrict__ rhs, BoxDev b, Background bg, Options o,
@@ -756,7 +756,8 @@ __global__ void __launch_bounds__(kTB *kTB, kMinBlocks<T>)
             double *__restrict__ mdot_part)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    faces_tile<T, MDOT>(prim, src, rhs, b, bg, o, idx0_, idx1_, idx2_, zchunk,
+    faces_tile<T, MDOT, false, BGK>(prim, src, rhs, b, bg, o, idx0_, idx1_,
+                                    idx2_, zchunk,
                         blockIdx.x, blockIdx.y, blockIdx.z, smem_raw,
                         mdot_part,
                         blockIdx.x + (int64_t)gridDim.x *
@@ -1012,7 +1013,7 @@ __device__ __forceinline__ void flush_max(DevStatus *st, double v)
 // 942-969).  The stage input k, the primitive cache and the sources are of
 // type T; U, the accumulator and con2prim are FP64.  The mixed path starts
 // con2prim from the primitive cache's pressure of the same cell.
-template <int MODE, typename T, bool CG = false>
+template <int MODE, typename T, bool CG = false, int BGK = -1>
 __device__ __forceinline__ void
 stage_item(const double *un, int64_t ucs, const double *us, int64_t tcs,
            double *out, int64_t ocs, const T *__restrict__ kv,
@@ -1076,9 +1077,9 @@ stage_item(const double *un, int64_t ucs, const double *us, int64_t tcs,
         cell_xyz(o, i, j, k, x, y, z);
         GeoFullT<T> f;
         if (prep && o.use_src)
-            metric_T<T, true>(bg, x, y, z, f.g, &f);
+            metric_T<T, true, BGK>(bg, x, y, z, f.g, &f);
         else
-            metric_T<T, false>(bg, x, y, z, f.g, nullptr);
+            metric_T<T, false, BGK>(bg, x, y, z, f.g, nullptr);
         double gLL[6];
         gLL_double(f.g, gLL);
         const double p_guess =
@@ -1157,7 +1158,7 @@ stage_item(const double *un, int64_t ucs, const double *us, int64_t tcs,
     }
 }
 
-template <int MODE, typename T>
+template <int MODE, typename T, int BGK>
 __global__ void __launch_bounds__(256, kMinBlocks<T>)
     k_stage(const double *un, int64_t ucs, const double *us, int64_t tcs,
             double *out, int64_t ocs, const T *__restrict__ kv,
@@ -1179,7 +1180,8 @@ __global__ void __launch_bounds__(256, kMinBlocks<T>)
     {
         double cell_inv = 0.0;
         if (t < n)
-            stage_item<MODE, T>(un, ucs, us, tcs, out, ocs, kv, acc, prim, src,
+            stage_item<MODE, T, false, BGK>(un, ucs, us, tcs, out, ocs, kv, acc,
+                                            prim, src,
                                 b, bg, o, stage, dt, prep, store_p, cfl != 0,
                                 inv, st, t, cnt, cell_inv);
         flush_counts(st, cnt);
@@ -2085,18 +2087,21 @@ cudaError_t configure_kernels()
 {
     cudaError_t e = cudaSuccess;
     const cudaFuncAttribute attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_faces<double, false>, attr,
-                                 (int)faces_smem<double>());
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_faces<double, true>, attr,
-                                 (int)faces_smem<double>());
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_faces<float, false>, attr,
-                                 (int)faces_smem<float>());
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_faces<float, true>, attr,
-                                 (int)faces_smem<float>());
+    const int d = (int)faces_smem<double>(), f = (int)faces_smem<float>();
+    const void *fp64[] = {(const void *)k_faces<double, false, 0>,
+                          (const void *)k_faces<double, true, 0>,
+                          (const void *)k_faces<double, false, 1>,
+                          (const void *)k_faces<double, true, 1>};
+    const void *fp32[] = {(const void *)k_faces<float, false, 0>,
+                          (const void *)k_faces<float, true, 0>,
+                          (const void *)k_faces<float, false, 1>,
+                          (const void *)k_faces<float, true, 1>};
+    for (const void *k : fp64)
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k, attr, d);
+    for (const void *k : fp32)
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k, attr, f);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_ensemble<double>, attr,
                                  (int)faces_smem<double>());
@@ -2179,14 +2184,18 @@ void launch_faces(const T *prim, const T *src, T *rhs, const BoxDev &b,
     dim3 grid((b.in[0] + kTC - 1) / kTC, (b.in[1] + kTC - 1) / kTC,
               (b.in[2] + zchunk - 1) / zchunk);
     dim3 block(kTB, kTB);
-    if (o.accretion_radius > 0.0 && mdot_part)
-        k_faces<T, true><<<grid, block, faces_smem<T>(), s>>>(
+    // one instantiation per background kind: each carries only its own
+    // metric code
+    const bool md = o.accretion_radius > 0.0 && mdot_part;
+    auto go = [&](auto kern) {
+        kern<<<grid, block, faces_smem<T>(), s>>>(
             prim, src, rhs, b, bg, o, inv_dx[0], inv_dx[1], inv_dx[2], zchunk,
-            mdot_part);
+            md ? mdot_part : nullptr);
+    };
+    if (bg.kind == 1)
+        md ? go(k_faces<T, true, 1>) : go(k_faces<T, false, 1>);
     else
-        k_faces<T, false><<<grid, block, faces_smem<T>(), s>>>(
-            prim, src, rhs, b, bg, o, inv_dx[0], inv_dx[1], inv_dx[2], zchunk,
-            nullptr);
+        md ? go(k_faces<T, true, 0>) : go(k_faces<T, false, 0>);
 }
 
 void launch_mdot_sum(const double *part, int64_t n, double weight,
@@ -2222,18 +2231,18 @@ void launch_stage(int mode, const double *un, int64_t ucs, const double *us,
     const double i0 = inv_dx ? inv_dx[0] : 0.0, i1 = inv_dx ? inv_dx[1] : 0.0,
                  i2 = inv_dx ? inv_dx[2] : 0.0;
     const int pf = prep, cf = cfl ? 1 : 0;
+    auto go = [&](auto kern) {
+        kern<<<grid, 256, 0, s>>>(un, ucs, us, tcs, out, ocs, k, acc, prim, src,
+                                  b, bg, o, stage, dt, pf, cf, i0, i1, i2, st);
+    };
+    // one instantiation per background kind (only its own metric code)
+    const bool pn = bg.kind == 1;
     if (mode == 0)
-        k_stage<0, T><<<grid, 256, 0, s>>>(un, ucs, us, tcs, out, ocs, k, acc,
-                                           prim, src, b, bg, o, stage, dt, pf,
-                                           cf, i0, i1, i2, st);
+        pn ? go(k_stage<0, T, 1>) : go(k_stage<0, T, 0>);
     else if (mode == 1)
-        k_stage<1, T><<<grid, 256, 0, s>>>(un, ucs, us, tcs, out, ocs, k, acc,
-                                           prim, src, b, bg, o, stage, dt, pf,
-                                           cf, i0, i1, i2, st);
+        pn ? go(k_stage<1, T, 1>) : go(k_stage<1, T, 0>);
     else
-        k_stage<2, T><<<grid, 256, 0, s>>>(un, ucs, us, tcs, out, ocs, k, acc,
-                                           prim, src, b, bg, o, stage, dt, pf,
-                                           cf, i0, i1, i2, st);
+        pn ? go(k_stage<2, T, 1>) : go(k_stage<2, T, 0>);
 }
 
 void launch_max_inv_dt(const double *state, const BoxDev &b,
