@@ -624,6 +624,9 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--adjoint-only", action="store_true",
                     help="run only the adjoint leg and print its JSON")
+    ap.add_argument("--widened-only", action="store_true",
+                    help="run only the legs beyond the step and print their "
+                         "JSON")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -666,6 +669,18 @@ def main():
         print(json.dumps({"adjoint": run_adjoint(
             args.adjoint_n, args.adjoint_steps, args.adjoint_every,
             args.adjoint_fd_steps, None)}), flush=True)
+        return
+
+    if args.widened_only:
+        import torch
+        torch.cuda.set_device(local_rank)
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except (OSError, ValueError):
+            pass
+        print(json.dumps({"widened": run_widened(
+            peaks.get("hbm_gbs", 6650.0))}), flush=True)
         return
 
     if world > 1:

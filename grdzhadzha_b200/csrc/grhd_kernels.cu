@@ -1851,7 +1851,7 @@ __device__ __forceinline__ double log_sqrt_det6(const double *g)
 // finite-difference derivatives (add_static_metric_sources_to_conserved_rhs,
 // :367-427; one-sided where a neighbour's stored primitives are metric-
 // source atmosphere, make_metric_source_derivative_stencil, :283-322).
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
     k_ccz4_rhs(const double *__restrict__ s, BoxDev b, Options o,
                const double *__restrict__ prim, const double *__restrict__ gc,
                double *__restrict__ rhs, int64_t rcs, double inv0,
