@@ -576,6 +576,20 @@ def run_widened(hbm_peak):
         "note": "7 state components read per cell; includes the host sum"}
     del boxes, stages, lv, op
     torch.cuda.empty_cache()
+    # the binary-disk configuration (circumbinary Keplerian disk on the
+    # time-dependent PN metric), 320^3 mixed, 3 RK4 steps
+    op, lv = W.binary_disk(320, precision="mixed")
+    st = {"t": 0.0, "mi": 0.0}
+
+    def disk_steps():
+        st["t"], st["mi"], _ = op.advance_rk4_cfl_steps(
+            lv, CFL, 3, time=st["t"], max_inverse_dt=st["mi"])
+    ms = _time(disk_steps, reps=2, warmup=1) / 3.0
+    out["binary_disk_320_mixed"] = {
+        "value": lv.num_cells / (ms / 1e3), "unit": "cell-updates/s",
+        "ms_per_step": ms, "note": "RK4, CFL 0.25, volume-time source on"}
+    del op, lv
+    torch.cuda.empty_cache()
     # KITP source terms on a binary-PN disk, 128^3
     n = 128
     op, lv = W.binary_pn_disk(n)

@@ -117,6 +117,16 @@ class Error(C.Structure):
 _P = C.POINTER
 _dp = _P(C.c_double)
 _vp = C.c_void_p
+class KitpDiskConfig(C.Structure):
+    _fields_ = [("mach", C.c_double), ("aspect_ratio", C.c_double),
+                ("cavity_radius_factor", C.c_double),
+                ("cavity_delta", C.c_double),
+                ("outer_cutoff_radius", C.c_double),
+                ("rho_peak", C.c_double),
+                ("mode_amplitude", C.c_double * 4),
+                ("mode_phase", C.c_double * 4)]
+
+
 class CheckpointHeader(C.Structure):
     """grhd_checkpoint_header (the KITPCHK1 header fields)."""
     _fields_ = [("num_components", C.c_int), ("num_cells", C.c_int),
@@ -234,6 +244,10 @@ SIGNATURES = {
                                                    _P(Box), _dp, _dp, _vp]),
     "grhd_ccz4_advance_ssprk2": (C.c_int, [_vp, _vp, C.c_int64, _P(Box), _dp,
                                            C.c_double, _P(Diagnostics), _vp]),
+    "grhd_default_kitp_disk_config": (None, [_P(KitpDiskConfig)]),
+    "grhd_kitp_disk_initial_data": (C.c_int, [_vp, _vp, C.c_int64, _P(Box),
+                                              _P(KitpDiskConfig), C.c_double,
+                                              _vp]),
     "grhd_region_copy": (C.c_int, [C.c_int, _vp, C.c_int64, _P(Box),
                                    _P(C.c_int), _P(C.c_int), _vp, _vp]),
     "grhd_checkpoint_write": (C.c_int, [C.c_char_p, _P(CheckpointHeader),

@@ -1805,6 +1805,72 @@ int grhd_region_copy(int pack, double *state, int64_t state_cs,
     return cudaGetLastError() == cudaSuccess ? GRHD_OK : GRHD_ERR_CUDA;
 }
 
+void grhd_default_kitp_disk_config(grhd_kitp_disk_config *c)
+{
+    if (!c)
+        return;
+    // SimulationConfig, Main_GRHDLevelDataBinaryPNKITPDisk.cpp:56-61
+    c->mach = 10.0;
+    c->aspect_ratio = 0.1;
+    c->cavity_radius_factor = 2.5;
+    c->cavity_delta = 1.0e-5;
+    c->outer_cutoff_radius = 1.0e10;
+    c->rho_peak = 4.0e-5;
+    for (int m = 0; m < 4; ++m)
+        c->mode_amplitude[m] = c->mode_phase[m] = 0.0;
+}
+
+int grhd_kitp_disk_initial_data(grhd_ctx *ctx, double *state,
+                                int64_t state_cs, const grhd_box *box,
+                                const grhd_kitp_disk_config *cfg, double time,
+                                void *stream)
+{
+    int st = common_checks(ctx, state, box);
+    if (st)
+        return st;
+    if (!cfg || !(cfg->mach > 0.0) || !(cfg->rho_peak > 0.0))
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, nullptr,
+                         0.0, "disk configuration needs mach > 0 and "
+                              "rho_peak > 0");
+    if (ctx->params.background != GRHD_BG_BINARY_PN)
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, nullptr,
+                         0.0, "the disk needs the binary post-Newtonian "
+                              "background");
+    const BoxDev b = make_box(box, state_cs);
+    if ((st = check_strides(ctx, b, state_cs, -1)))
+        return st;
+    const grhd_params &p = ctx->params;
+    KitpDiskDev k;
+    k.mach = cfg->mach;
+    k.aspect = cfg->aspect_ratio;
+    k.cavity_factor = cfg->cavity_radius_factor;
+    k.cavity_delta = cfg->cavity_delta;
+    k.outer_cutoff = cfg->outer_cutoff_radius;
+    k.rho_peak = cfg->rho_peak;
+    for (int m = 0; m < 4; ++m)
+    {
+        k.amp[m] = cfg->mode_amplitude[m];
+        k.phase[m] = cfg->mode_phase[m];
+    }
+    k.sep = p.pn_separation;
+    k.mass[0] = p.pn_mass_1;
+    k.mass[1] = p.pn_mass_2;
+    k.soft = p.pn_softening_radius;
+    const double total = p.pn_mass_1 + p.pn_mass_2;
+    k.omega_bin = p.pn_angular_velocity != 0.0
+                      ? p.pn_angular_velocity
+                      : std::sqrt(total / (p.pn_separation * p.pn_separation *
+                                           p.pn_separation));
+    double v1[3], v2[3];
+    pn_state(p, time, k.body[0], k.body[1], v1, v2);
+    cudaStream_t s = (cudaStream_t)stream;
+    ++ctx->launches;
+    launch_kitp_disk_fill(state, b, make_background(p, time), ctx->opt, k, s);
+    GRHD_CUDA(ctx, cudaGetLastError());
+    GRHD_CUDA(ctx, cudaStreamSynchronize(s));
+    return GRHD_OK;
+}
+
 int grhd_checkpoint_write(const char *path, const grhd_checkpoint_header *h,
                           const char *signature, const double *state,
                           int64_t state_cs, const grhd_box *box, char *err,

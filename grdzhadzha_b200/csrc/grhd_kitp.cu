@@ -192,6 +192,97 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// kitp_primitive (:465-520); the modes scale the midplane surface density.
+__device__ Prim kitp_disk_prim(const KitpDiskDev &k, const Options &o,
+                               const double pos[3], const Geo &g)
+{
+    Prim pr = atmosphere(o);
+    const double radius = sqrt(pos[0] * pos[0] + pos[1] * pos[1]);
+    if (radius <= 1.0e-12)
+        return pr;
+    const double phi = atan2(pos[1], pos[0]);
+    const double h = fmax(k.aspect * radius, 1.0e-12);
+    const double vprof = exp(-0.5 * (pos[2] / h) * (pos[2] / h));
+    const double zero_sigma = o.rho_floor / k.rho_peak;
+    // kitp_sigma_midplane (:408-418) with stable_logistic_cutoff (:398-406)
+    const double safe_r = fmax(radius, 1.0e-12);
+    const double cavity = k.cavity_factor * k.sep;
+    const double cprof =
+        (1.0 - k.cavity_delta) * exp(-pow(cavity / safe_r, 12.0)) +
+        k.cavity_delta;
+    const double arg = -2.0 * (radius - k.outer_cutoff);
+    const double cut =
+        arg > 700.0 ? 1.0 : (arg < -700.0 ? 0.0 : 1.0 - 1.0 / (1.0 + exp(arg)));
+    double sigma = cprof * cut;
+    double modes = 1.0;
+    for (int m = 0; m < 4; ++m)
+        modes += k.amp[m] * cos((m + 1) * phi + k.phase[m]);
+    sigma *= modes;
+    pr.rho = fmax(o.rho_floor, k.rho_peak * (sigma * vprof + zero_sigma));
+    // binary_point_mass_potential (:444-463)
+    double pot = 0.0;
+    for (int b = 0; b < 2; ++b)
+    {
+        double r2 = k.soft * k.soft;
+        for (int d = 0; d < 3; ++d)
+        {
+            const double dd = pos[d] - k.body[b][d];
+            r2 += dd * dd;
+        }
+        pot -= k.mass[b] / sqrt(r2);
+    }
+    const double cs2 =
+        fmax(o.p_floor / pr.rho, -pot / (k.mach * k.mach));
+    pr.p = fmax(o.p_floor, pr.rho * cs2 / o.G);
+    pr.eps = pr.p / ((o.G - 1.0) * pr.rho);
+    // kitp_radial_velocity (:420-427), kitp_phi_velocity (:429-442)
+    const double v0 = 1.0e-4 * k.omega_bin * k.sep;
+    const double vr = v0 * sin(phi) * (radius / k.sep) *
+                      exp(-pow(radius / (3.5 * k.sep), 6.0));
+    const double total = k.mass[0] + k.mass[1];
+    const double wg = sqrt(total / (safe_r * safe_r * safe_r) *
+                           fmax(0.0, 1.0 - 1.0 / (k.mach * k.mach)));
+    double vphi = 0.0;
+    if (wg > 0.0)
+        vphi = pow(pow(k.omega_bin, -4.0) + pow(wg, -4.0), -0.25) * safe_r;
+    const double cv[3] = {vr * cos(phi) - vphi * sin(phi),
+                          vr * sin(phi) + vphi * cos(phi), 0.0};
+    for (int d = 0; d < 3; ++d)
+        pr.v[d] = (cv[d] + g.shift[d]) / g.lapse;
+    floors(o, pr, g.gLL);
+    return pr;
+}
+
+// fill_kitp_level_data (:522-555): every ghosted cell.
+__global__ void __launch_bounds__(256)
+    k_kitp_disk_fill(double *__restrict__ s, BoxDev b, Background bg,
+                     Options o, KitpDiskDev k)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+         t < b.gvol(); t += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int i = b.glo[0] + (int)(t % b.gn[0]);
+        const int64_t r = t / b.gn[0];
+        const int j = b.glo[1] + (int)(r % b.gn[1]);
+        const int l = b.glo[2] + (int)(r / b.gn[1]);
+        double pos[3];
+        cell_xyz(o, i, j, l, pos[0], pos[1], pos[2]);
+        Geo g;
+        background_metric<false>(bg, pos[0], pos[1], pos[2], g, nullptr);
+        const Prim pr = kitp_disk_prim(k, o, pos, g);
+        s[kRho * b.cs + t] = pr.rho;
+        s[kEps * b.cs + t] = pr.eps;
+        s[kPress * b.cs + t] = pr.p;
+        for (int d = 0; d < 3; ++d)
+            s[(kV1 + d) * b.cs + t] = pr.v[d];
+        const Cons c = p2c(pr, g.gLL);
+        s[kD * b.cs + t] = c.D;
+        s[kTau * b.cs + t] = c.tau;
+        for (int d = 0; d < 3; ++d)
+            s[(kS1 + d) * b.cs + t] = c.S[d];
+    }
+}
+
 int blocks_for(int64_t n)
 {
     int64_t g = (n + 255) / 256;
@@ -223,6 +314,13 @@ void launch_kitp_sink_decay(double *state, const BoxDev &b, const Options &o,
 {
     k_kitp_sink_decay<<<blocks_for(b.ivol()), 256, 0, s>>>(state, b, o, k,
                                                            dt);
+}
+
+void launch_kitp_disk_fill(double *state, const BoxDev &b,
+                           const Background &bg, const Options &o,
+                           const KitpDiskDev &k, cudaStream_t s)
+{
+    k_kitp_disk_fill<<<blocks_for(b.gvol()), 256, 0, s>>>(state, b, bg, o, k);
 }
 
 } // namespace grhd

@@ -33,4 +33,21 @@ void launch_kitp_sink_rhs(double *rhs, int64_t rcs, const double *state,
 void launch_kitp_sink_decay(double *state, const BoxDev &b, const Options &o,
                             const KitpDev &k, double dt, cudaStream_t s);
 
+// The disk drivers' Keplerian disk (kitp_primitive, :398-520) with the
+// azimuthal density modes m = 1..4 (new): the binary (masses, separation,
+// softening, orbital frequency, body positions at the fill time) and the
+// disk settings of SimulationConfig (:56-61).
+struct KitpDiskDev
+{
+    double mach, aspect, cavity_factor, cavity_delta, outer_cutoff, rho_peak;
+    double amp[4], phase[4];
+    double sep, mass[2], soft, omega_bin;
+    double body[2][3];
+};
+
+// Primitives and conserved variables of every ghosted cell.
+void launch_kitp_disk_fill(double *state, const BoxDev &b,
+                           const Background &bg, const Options &o,
+                           const KitpDiskDev &k, cudaStream_t s);
+
 } // namespace grhd

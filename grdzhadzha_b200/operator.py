@@ -434,6 +434,27 @@ class _OperatorBase:
             self._ctx, _ptr(state.state), state.comp_stride(), C.byref(b),
             C.byref(c), _stream()))
 
+    def fill_kitp_disk(self, state: LevelBox, time=0.0, **config):
+        """The binary disk drivers' Keplerian disk (kitp_primitive +
+        fill_kitp_level_data, Main_GRHDLevelDataBinaryPNKITPDisk.cpp:
+        398-555) on the device, SimulationConfig defaults (:56-61) with
+        `config` overrides (mach, aspect_ratio, cavity_radius_factor,
+        cavity_delta, outer_cutoff_radius, rho_peak, mode_amplitude[4],
+        mode_phase[4]); needs the CircularBinaryPN background."""
+        c = L.KitpDiskConfig()
+        self._lib.grhd_default_kitp_disk_config(C.byref(c))
+        for k, v in config.items():
+            if k in ("mode_amplitude", "mode_phase"):
+                arr = getattr(c, k)
+                for i, x in enumerate(v):
+                    arr[i] = x
+            else:
+                setattr(c, k, v)
+        b = state.c_box()
+        self._check(self._lib.grhd_kitp_disk_initial_data(
+            self._ctx, _ptr(state.state), state.comp_stride(), C.byref(b),
+            C.byref(c), time, _stream()))
+
     def perturb_density(self, state: LevelBox, amplitude, seed, time=0.0):
         b = state.c_box()
         self._check(self._lib.grhd_perturb_density(

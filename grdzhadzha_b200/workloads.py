@@ -77,6 +77,40 @@ def binary_pn_disk(n, half_width=40.0, gamma=5.0 / 3.0, inner_radius=14.0,
     return op, lv
 
 
+def binary_disk(n=320, half_width=60.0, gamma=5.0 / 3.0, inner_radius=20.0,
+                outer_radius=50.0, aspect_ratio=0.1, mode_amplitude=1e-3,
+                seed=SEED + 2, precision="mixed", device="cuda"):
+    """The binary-disk configuration: circular PN binary (0.5 + 0.5,
+    separation 10, softening 0.5, Newtonian orbital frequency) with the disk
+    drivers' Keplerian disk (kitp_primitive) between inner_radius (the
+    cavity edge, 2 separations) and outer_radius (the logistic cut-off),
+    H/R = aspect_ratio (Mach 1 / aspect_ratio), and azimuthal density
+    modes m = 1..4 of amplitude mode_amplitude with phases U[0, 2 pi)
+    (numpy, seeded); n^3 over [-half_width, half_width]^3, atmosphere
+    1e-10 / 8e-14 / v^2 cap 0.72 and recovery floor 8e-14 / v^2 cap 0.75
+    (the driver's, make_recovery_options, :339-346), MUSCL-MC (theta 1.3) +
+    HLLE, volume-time source on.  Returns (operator, level)."""
+    nn = (n, n, n) if isinstance(n, int) else tuple(n)
+    dx = 2.0 * half_width / nn[0]
+    c = tuple(0.5 * nn[d] * dx for d in range(3))
+    sep = 10.0
+    op = TimeDependentFixedBGLevelDataFiniteVolumeOperator(
+        IdealGasEOS(gamma),
+        CircularBinaryPN(mass_1=0.5, mass_2=0.5, separation=sep,
+                         softening_radius=0.5, dx=dx),
+        dx, c, AtmosphereOptions(1e-10, 8e-14, 0.72), 1.3, True,
+        RecoveryOptions(80, 1e-12, 8e-14, 0.75), True, True, 1e-3, 0.0, 0.0,
+        precision)
+    rng = np.random.default_rng(seed)
+    lv = LevelBox.cube(nn, device=device)
+    op.fill_kitp_disk(lv, mach=1.0 / aspect_ratio, aspect_ratio=aspect_ratio,
+                      cavity_radius_factor=inner_radius / sep,
+                      outer_cutoff_radius=outer_radius,
+                      mode_amplitude=[mode_amplitude] * 4,
+                      mode_phase=list(rng.uniform(0.0, 2.0 * np.pi, 4)))
+    return op, lv
+
+
 def michel(n, sonic_radius=8.0, half_width=16.0, gamma=4.0 / 3.0,
            noise=1e-6, seed=SEED, accretion_radius=0.0, precision="fp64",
            device="cuda"):

@@ -499,6 +499,30 @@ int grhd_region_copy(int pack, double *state, int64_t state_comp_stride,
                      const grhd_box *box, const int lo[3], const int hi[3],
                      double *buffer, void *stream);
 
+/* The binary disk drivers' Keplerian disk (kitp_primitive +
+ * fill_kitp_level_data, Main_GRHDLevelDataBinaryPNKITPDisk.cpp:398-555),
+ * the initial data of the benchmark's binary-disk configuration: the
+ * SimulationConfig disk settings (:56-61) and, new, azimuthal density
+ * modes m = 1..4 (surface density times 1 + sum_m A_m cos(m phi + phase_m)).
+ * The operator's background must be the binary PN one; its binary
+ * (masses, separation, orbital frequency, phase, time, softening) and
+ * atmosphere floors are the disk's. */
+typedef struct grhd_kitp_disk_config
+{
+    double mach, aspect_ratio, cavity_radius_factor, cavity_delta,
+        outer_cutoff_radius, rho_peak;
+    double mode_amplitude[4], mode_phase[4];
+} grhd_kitp_disk_config;
+/* The driver's defaults (mach 10, H/R 0.1, cavity 2.5 separations with
+ * floor 1e-5, no outer cut-off, rho_peak 4e-5), no modes. */
+void grhd_default_kitp_disk_config(grhd_kitp_disk_config *config);
+/* Primitives and conserved variables over the ghosted box at `time`. */
+int grhd_kitp_disk_initial_data(grhd_ctx *ctx, double *state,
+                                int64_t state_comp_stride,
+                                const grhd_box *box,
+                                const grhd_kitp_disk_config *config,
+                                double time, void *stream);
+
 /* The header of a KITPCHK1 checkpoint (write_checkpoint /
  * read_checkpoint_header, Examples/GRHDLevelDataBinaryPNKITPDisk/
  * Main_GRHDLevelDataBinaryPNKITPDisk.cpp:1289-1505).  num_components is

@@ -3122,3 +3122,117 @@ void orc_ccz4_fill_from_background(const orc_params *p, const orc_box *b,
                     s[(CZ_SHIFT + a) * cs + idx] = v.shift[a];
             }
 }
+
+/* ------------------------------------------------------------------------ */
+/* The binary disk drivers' Keplerian disk (kitp_primitive and               */
+/* fill_kitp_level_data, Examples/GRHDLevelDataBinaryPNKITPDisk/             */
+/* Main_GRHDLevelDataBinaryPNKITPDisk.cpp:398-555), on the operator's binary */
+/* (masses, separation, phase, time, softening of orc_params) and its        */
+/* atmosphere floors, plus the azimuthal density modes m = 1..4 of the       */
+/* benchmark's binary-disk configuration (new).                              */
+/* ------------------------------------------------------------------------ */
+
+/* stable_logistic_cutoff, :398-406 */
+static double kitp_cutoff(double radius, double outer_radius)
+{
+    const double arg = -2.0 * (radius - outer_radius);
+    if (arg > 700.0)
+        return 1.0;
+    if (arg < -700.0)
+        return 0.0;
+    return 1.0 - 1.0 / (1.0 + exp(arg));
+}
+
+static double kitp_omega_bin(const orc_params *p)
+{
+    const double total = p->pn_mass_1 + p->pn_mass_2;
+    return p->pn_angular_velocity != 0.0
+               ? p->pn_angular_velocity
+               : sqrt(total / (p->pn_separation * p->pn_separation *
+                               p->pn_separation));
+}
+
+/* kitp_primitive, :465-520, with the modes applied to the density profile
+ * (1 + sum_m A_m cos(m phi + phase_m)) before the floor. */
+static Prim kitp_disk_prim(const orc_params *p, const orc_kitp_disk *k,
+                           const double pos[3], const double body[2][3],
+                           const Geom *g)
+{
+    Prim pr = atmosphere_prim(p);
+    const double radius = sqrt(pos[0] * pos[0] + pos[1] * pos[1]);
+    if (radius <= 1.0e-12)
+        return pr;
+    const double phi = atan2(pos[1], pos[0]);
+    const double h = dmax(k->aspect_ratio * radius, 1.0e-12);
+    const double vprof = exp(-0.5 * (pos[2] / h) * (pos[2] / h));
+    const double zero_sigma = p->atmo_rho_floor / k->rho_peak;
+    /* kitp_sigma_midplane, :408-418 */
+    const double safe_r = dmax(radius, 1.0e-12);
+    const double cavity = k->cavity_radius_factor * p->pn_separation;
+    const double cprof =
+        (1.0 - k->cavity_delta) * exp(-pow(cavity / safe_r, 12.0)) +
+        k->cavity_delta;
+    double sigma = cprof * kitp_cutoff(radius, k->outer_cutoff_radius);
+    double modes = 1.0;
+    for (int m = 0; m < 4; ++m)
+        modes += k->mode_amplitude[m] * cos((m + 1) * phi + k->mode_phase[m]);
+    sigma *= modes;
+    const double dscale = sigma * vprof + zero_sigma;
+    pr.rho = dmax(p->atmo_rho_floor, k->rho_peak * dscale);
+    /* binary_point_mass_potential, :444-463 */
+    const double masses[2] = {p->pn_mass_1, p->pn_mass_2};
+    double pot = 0.0;
+    for (int b = 0; b < 2; ++b)
+    {
+        double r2 = p->pn_softening_radius * p->pn_softening_radius;
+        for (int d = 0; d < 3; ++d)
+        {
+            const double dd = pos[d] - body[b][d];
+            r2 += dd * dd;
+        }
+        pot -= masses[b] / sqrt(r2);
+    }
+    const double cs2 = dmax(p->atmo_pressure_floor / pr.rho,
+                            -pot / (k->mach * k->mach));
+    pr.p = dmax(p->atmo_pressure_floor, pr.rho * cs2 / p->gamma);
+    pr.eps = pr.p / ((p->gamma - 1.0) * pr.rho);
+    /* kitp_radial_velocity, :420-427; kitp_phi_velocity, :429-442 */
+    const double wb = kitp_omega_bin(p);
+    const double sep = p->pn_separation;
+    const double v0 = 1.0e-4 * wb * sep;
+    const double vr = v0 * sin(phi) * (radius / sep) *
+                      exp(-pow(radius / (3.5 * sep), 6.0));
+    const double total = p->pn_mass_1 + p->pn_mass_2;
+    const double wg = sqrt(total / (safe_r * safe_r * safe_r) *
+                           dmax(0.0, 1.0 - 1.0 / (k->mach * k->mach)));
+    double vphi = 0.0;
+    if (wg > 0.0)
+        vphi = pow(pow(wb, -4.0) + pow(wg, -4.0), -0.25) * safe_r;
+    const double cv[3] = {vr * cos(phi) - vphi * sin(phi),
+                          vr * sin(phi) + vphi * cos(phi), 0.0};
+    for (int d = 0; d < 3; ++d)
+        pr.v[d] = (cv[d] + g->shift[d]) / g->lapse;
+    enforce_floors(p, &pr, g->gLL);
+    return pr;
+}
+
+void orc_fill_kitp_disk(const orc_params *p, const orc_kitp_disk *k,
+                        const orc_box *b, double *state, double t)
+{
+    double body[2][3], v1[3], v2[3];
+    pn_state(p, t, body[0], body[1], v1, v2);
+    for (int kk = b->glo[2]; kk <= b->ghi[2]; ++kk)
+        for (int j = b->glo[1]; j <= b->ghi[1]; ++j)
+            for (int i = b->glo[0]; i <= b->ghi[0]; ++i)
+            {
+                double pos[3];
+                cell_position(p, i, j, kk, &pos[0], &pos[1], &pos[2]);
+                Geom g;
+                load_geometry(p, t, i, j, kk, &g);
+                const Prim pr = kitp_disk_prim(p, k, pos, body, &g);
+                const int64_t idx = fab_index(b, i, j, kk);
+                store_prim(b, state, idx, &pr);
+                const Cons c = p2c(p->gamma, &pr, g.gLL);
+                store_cons(b, state, idx, &c);
+            }
+}

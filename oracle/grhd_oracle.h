@@ -266,6 +266,20 @@ void orc_kitp_sink_decay(const orc_params *p, const orc_kitp_config *k,
                          const orc_box *box, double *state, double t,
                          double dt);
 
+/* ---- the binary disk drivers' Keplerian disk (kitp_primitive,
+ * Main_GRHDLevelDataBinaryPNKITPDisk.cpp:398-555; SimulationConfig :56-61)
+ * with azimuthal density modes m = 1..4 (new) ---- */
+typedef struct orc_kitp_disk
+{
+    double mach, aspect_ratio, cavity_radius_factor, cavity_delta,
+        outer_cutoff_radius, rho_peak;
+    double mode_amplitude[4], mode_phase[4];
+} orc_kitp_disk;
+/* Primitives and conserved variables over the ghosted box at time t (the
+ * operator's binary and atmosphere floors). */
+void orc_fill_kitp_disk(const orc_params *p, const orc_kitp_disk *k,
+                        const orc_box *box, double *state, double t);
+
 /* ---- the operator on CCZ4-stored geometry (LevelDataFiniteVolumeOperator,
  * Source/Matter/GRHD/FArrayBoxFiniteVolume.hpp:681-1364) ----
  * state: 36 components of comp_stride each, GRChombo's 25 CCZ4 variables

@@ -96,6 +96,16 @@ class MichelConfig(C.Structure):
         "atmosphere_radius", "root_tolerance")]
 
 
+class KitpDisk(C.Structure):
+    _fields_ = [("mach", C.c_double), ("aspect_ratio", C.c_double),
+                ("cavity_radius_factor", C.c_double),
+                ("cavity_delta", C.c_double),
+                ("outer_cutoff_radius", C.c_double),
+                ("rho_peak", C.c_double),
+                ("mode_amplitude", C.c_double * 4),
+                ("mode_phase", C.c_double * 4)]
+
+
 _lib = None
 
 
@@ -200,6 +210,9 @@ def lib():
         L.orc_kitp_sink_rhs.argtypes = [P, K, B, dp, dp, i64, C.c_double]
         L.orc_kitp_sink_decay.argtypes = [P, K, B, dp, C.c_double,
                                           C.c_double]
+        L.orc_fill_kitp_disk.argtypes = [P, C.POINTER(KitpDisk), B, dp,
+                                         C.c_double]
+        L.orc_fill_kitp_disk.restype = None
         L.orc_ccz4_compute_rhs.argtypes = [P, B, dp, dp, i64, dp,
                                            C.POINTER(Error)]
         L.orc_ccz4_recover_primitives.argtypes = [P, B, dp, C.POINTER(Diag)]
@@ -589,3 +602,22 @@ def ccz4_max_inverse_dt(p, box, state36):
     if st:
         raise OracleError(st, err)
     return out.value
+
+
+def kitp_disk(**kw) -> KitpDisk:
+    """The disk drivers' SimulationConfig disk defaults (:56-61), no modes,
+    with overrides."""
+    k = KitpDisk(10.0, 0.1, 2.5, 1e-5, 1e10, 4e-5)
+    for name, v in kw.items():
+        if name in ("mode_amplitude", "mode_phase"):
+            arr = getattr(k, name)
+            for i, x in enumerate(v):
+                arr[i] = x
+        else:
+            setattr(k, name, v)
+    return k
+
+
+def fill_kitp_disk(p, k, box, state, t=0.0):
+    lib().orc_fill_kitp_disk(C.byref(p), C.byref(k), C.byref(box), _dp(state),
+                             t)

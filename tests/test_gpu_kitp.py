@@ -4,7 +4,12 @@ on the GPU against the oracle's restatement: the alpha-viscosity stress
 divergence (:676-806), the sink right-hand side (:567-610) and the sink
 decay (:612-662), on the binary-PN disk of Examples/GRHDLevelDataBinaryPNDisk
 (56^2 x 9).  Per component, max|GPU - oracle| <= 1e-12 of max|oracle|
-(the device's exp / pow / division round differently from libm's)."""
+(the device's exp / pow / division round differently from libm's).
+
+Also the driver's Keplerian disk (kitp_primitive, :398-520) as initial data
+of the benchmark's binary-disk configuration: its GPU fill against the
+oracle, that configuration's RHS against the oracle, and the configuration
+at its full 320^3 in mixed precision against FP64."""
 import numpy as np
 import pytest
 
@@ -70,3 +75,84 @@ def test_requires_binary_background():
     lv = cases.gpu_level(box, s)
     with pytest.raises(InvalidArgument):
         op.kitp_sink_decay(lv, 0.0, 0.1)
+
+
+# ---- the disk drivers' Keplerian disk (kitp_primitive) and the binary-disk
+# configuration built on it
+
+DISK = dict(mach=10.0, aspect_ratio=0.1, cavity_radius_factor=2.0,
+            outer_cutoff_radius=50.0, mode_amplitude=[1e-3] * 4,
+            mode_phase=[0.3, 1.7, 2.9, 4.4])
+
+
+def _disk_case(n=48, L=60.0, t=0.35):
+    dx = 2 * L / n
+    c = 0.5 * n * dx
+    p = O.default_params(background=O.BG_BINARY_PN, pn_mass_1=0.5,
+                         pn_mass_2=0.5, pn_separation=10.0,
+                         pn_softening_radius=0.5, gamma=5 / 3, dx=dx,
+                         center=(c, c, c), atmo_rho_floor=1e-10,
+                         atmo_pressure_floor=8e-14,
+                         atmo_max_velocity_squared=0.72,
+                         rec_max_velocity_squared=0.75, rec_max_iterations=80,
+                         rec_pressure_floor=8e-14,
+                         limiter_theta=1.3, use_metric_volume_time_sources=1)
+    box = O.make_box((n, n, n))
+    s = O.new_state(box)
+    O.fill_kitp_disk(p, O.kitp_disk(**DISK), box, s, t)
+    return p, box, s, t
+
+
+def test_kitp_disk_fill_matches_oracle():
+    """Primitives and conserved variables of every ghosted cell at a
+    binary phase off the axes: <= 1e-12 of each component's scale."""
+    p, box, s, t = _disk_case()
+    op = cases.gpu_operator(p)
+    lv = cases.gpu_level(box, np.zeros_like(s))
+    op.fill_kitp_disk(lv, time=t, **DISK)
+    err = cases.rel_err(lv.state.cpu().numpy().reshape(11, -1),
+                        s.reshape(11, -1))
+    print("disk fill err", err)
+    assert np.all(err <= 1e-12), err
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("mixed", 2e-3)])
+def test_binary_disk_rhs_matches_oracle(precision, tol):
+    """The binary-disk configuration's RHS (time-dependent metric with the
+    volume-time source) at 48^3: FP64 at the parity tolerance (measured on
+    B200: up to 6e-13); mixed within 2e-3 (measured 2.5e-5 to 1.4e-3: the
+    thin disk, H/R = 0.1, is near equilibrium, so its RHS is a small
+    residual of FP32 flux differences and FP32 metric-derivative sources,
+    tau the smallest of them; the tori's bound is 1e-4)."""
+    p, box, s, t = _disk_case()
+    op = cases.gpu_operator(p, precision=precision)
+    lv = cases.gpu_level(box, s)
+    rhs = lv.new_rhs()
+    op.compute_rhs(rhs, lv, time=t)
+    ref = O.compute_rhs(p, box, s.copy(), t)
+    err = cases.rel_err(rhs.cpu().numpy().reshape(5, -1), ref.reshape(5, -1))
+    print(f"binary disk RHS {precision}: {err}")
+    assert np.all(err <= tol), err
+
+
+def test_binary_disk_full_size_mixed_against_fp64():
+    """The binary-disk configuration at its full 320^3 (on [-60, 60]^3):
+    two RK4 steps of the mixed path against FP64 with the same dt, within
+    3e-6 of each conserved component's scale (measured on B200: D, S_i
+    0.9e-7 to 1.2e-7, tau 1.5e-6, the small residual of above), all
+    finite."""
+    from grdzhadzha_b200 import workloads as W
+    op64, a = W.binary_disk(320, precision="fp64")
+    opm, b = W.binary_disk(320, precision="mixed")
+    assert torch.equal(a.state, b.state)
+    dt = 0.5 * op64.compute_stable_dt(a, cfl=0.25)
+    t = 0.0
+    for _ in range(2):
+        op64.advance_rk4(a, time=t, dt=dt)
+        opm.advance_rk4(b, time=t, dt=dt)
+        t += dt
+    assert torch.isfinite(b.state).all()
+    err = cases.rel_err(b.interior(slice(0, 5)).cpu().numpy().reshape(5, -1),
+                        a.interior(slice(0, 5)).cpu().numpy().reshape(5, -1))
+    print("binary disk 320^3 mixed vs FP64 after 2 steps:", err)
+    assert np.all(err <= 3e-6), err
