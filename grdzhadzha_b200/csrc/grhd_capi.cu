@@ -35,6 +35,8 @@ struct grhd_ctx
     size_t int_cap = 0;      // doubles per interior buffer
     double *stage = nullptr; // 11 comps over the ghosted box
     size_t stage_cap = 0;
+    double *diag_part = nullptr;  // diagnostics: per-block partial results
+    size_t diag_cap = 0;
     double *ccz4_geo = nullptr;   // CCZ4 operator: geometry cache (16 comps)
     size_t ccz4_geo_cap = 0;
     double *ccz4_stage = nullptr; // CCZ4 operator: SSPRK2 stage (36 comps)
@@ -558,6 +560,7 @@ void grhd_destroy(grhd_ctx *ctx)
     cudaFree(ctx->flag);
     cudaFree(ctx->mdot_part);
     cudaFree(ctx->mdot_acc);
+    cudaFree(ctx->diag_part);
     cudaFree(ctx->ccz4_geo);
     cudaFree(ctx->ccz4_stage);
     if (ctx->status_h)
@@ -1698,16 +1701,17 @@ int grhd_disk_diagnostics(grhd_ctx *ctx, const double *state,
                          0.0, "state stride smaller than the ghosted box");
     cudaStream_t s = (cudaStream_t)stream;
     const int nb = diagnostics_blocks(b);
-    double *part = nullptr;
-    GRHD_CUDA(ctx, cudaMallocAsync((void **)&part, sizeof(double) * 7 * nb, s));
+    // the partial results live in the context (grown once), so that a call
+    // allocates nothing after the first on a box of its size
+    if ((st = grow(ctx, &ctx->diag_part, &ctx->diag_cap, (size_t)7 * nb)))
+        return st;
+    double *part = ctx->diag_part;
     ++ctx->launches;
     launch_diagnostics(state, b, make_background(ctx->params, time),
                        ctx->opt, part, s);
     std::vector<double> h((size_t)7 * nb);
     cudaError_t e = cudaMemcpyAsync(h.data(), part, sizeof(double) * 7 * nb,
                                     cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess)
-        e = cudaFreeAsync(part, s);
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(s);
     if (e != cudaSuccess)
