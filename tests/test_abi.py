@@ -49,3 +49,58 @@ def test_params_layout_matches_header_defaults():
     assert p.metric_time_derivative_step == 1e-3
     assert p.excision_radius == 0.0
     assert lib.grhd_status_string(1) == b"primitive recovery failed"
+
+
+# C struct of the header -> its ctypes mirror in grdzhadzha_b200._lib
+STRUCTS = {
+    "grhd_params": "Params", "grhd_box": "Box",
+    "grhd_diagnostics": "Diagnostics", "grhd_error": "Error",
+    "grhd_torus_config": "TorusConfig", "grhd_torus_params": "TorusParams",
+    "grhd_michel_config": "MichelConfig", "grhd_kitp_config": "KitpConfig",
+    "grhd_kitp_disk_config": "KitpDiskConfig",
+    "grhd_checkpoint_header": "CheckpointHeader",
+    "grhd_ensemble_member": "EnsembleMember",
+    "grhd_ensemble_tuning": "EnsembleTuning",
+    "grhd_adjoint_torus": "AdjointTorus",
+}
+
+
+def test_header_is_plain_c_and_ctypes_layouts_match(tmp_path):
+    """The header compiles as C99 and as C++, and every struct the ABI
+    passes has the same size and field offsets in C as in its ctypes
+    mirror (a mismatch would pass garbage across the boundary)."""
+    import shutil
+    import subprocess
+    from grdzhadzha_b200 import _lib as L
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    inc = os.path.join(ROOT, "include")
+    lines = ['#include <stdio.h>', '#include <stddef.h>',
+             '#include "grhd_b200.h"', 'int main(void) {']
+    for cname, pyname in STRUCTS.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in getattr(L, pyname)._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", '
+                         f'offsetof({cname}, {fname}));')
+    lines += ['return 0;', '}']
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Werror", "-I", inc,
+                    str(src), "-o", str(exe)], check=True)
+    gxx = shutil.which("g++")
+    if gxx is not None:
+        cpp = tmp_path / "layout.cpp"
+        cpp.write_text('#include "grhd_b200.h"\nint main() { return 0; }\n')
+        subprocess.run([gxx, "-std=c++17", "-fsyntax-only", "-Wall",
+                        "-Werror", "-I", inc, str(cpp)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True,
+                         text=True).stdout.split("\n")
+    for line in filter(None, out):
+        cname, what, value = line.split()
+        cls = getattr(L, STRUCTS[cname])
+        if what == "size":
+            assert C.sizeof(cls) == int(value), cname
+        else:
+            assert getattr(cls, what).offset == int(value), (cname, what)
