@@ -237,7 +237,7 @@ def run_ours(args, rank, world, local_rank):
     achieved = alg_bytes / (dom_ms / max(dom_n, 1) / 1e3) / 1e9
     # DRAM traffic per launch from the committed ncu capture of the same
     # kernel; a capture on a smaller grid is scaled by the cell count
-    traffic, traffic_note = None, None
+    traffic, traffic_note, fp64_pipe = None, None, None
     try:
         tr = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
         if tr.get("kernel_class") == dom:
@@ -245,6 +245,8 @@ def run_ours(args, rank, world, local_rank):
             traffic = tr["dram_bytes_per_launch"] * (n / g) ** 3
             traffic_note = (f"ncu capture at {g}^3 scaled by cells"
                             if g != n else "ncu capture")
+            if "fp64_pipe_active_pct" in tr:
+                fp64_pipe = tr["fp64_pipe_active_pct"] / 100.0
     except (OSError, ValueError, KeyError):
         pass
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved,
@@ -253,6 +255,9 @@ def run_ours(args, rank, world, local_rank):
                 "traffic_source": traffic_note, "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": alg_bytes,
                 "avg_launch_ms": dom_ms / max(dom_n, 1),
+                # the pipe that binds this kernel (ncu, committed capture):
+                # FP64 arithmetic, not HBM
+                "fp64_pipe_active_frac_ncu": fp64_pipe,
                 "step_frac_of_hbm_roofline":
                     value / world * BYTES_PER_CELL_UPDATE / 1e9 / hbm_peak}
     kernel_ms = {k: {"ms_total": v[0], "launches": v[1]}
