@@ -503,7 +503,7 @@ def _time(fn, reps=5, warmup=2):
 
 
 def run_widened(hbm_peak):
-    """The library paths beyond the north-star step, each timed on its own
+    """The library paths beyond the benchmarked step, each timed on its own
     (inputs larger than L2 except where stated): the operator on CCZ4-
     stored geometry, the multi-box level exchange, the split SSPRK2 of a
     multi-box level, the KITP disk-driver source terms, the diagnostics
