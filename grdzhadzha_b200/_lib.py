@@ -250,6 +250,14 @@ SIGNATURES = {
                                               _vp]),
     "grhd_region_copy": (C.c_int, [C.c_int, _vp, C.c_int64, _P(Box),
                                    _P(C.c_int), _P(C.c_int), _vp, _vp]),
+    "grhd_region_copy_components": (C.c_int, [C.c_int, _vp, C.c_int64,
+                                              _P(Box), _P(C.c_int),
+                                              _P(C.c_int), C.c_int, _vp,
+                                              _vp]),
+    "grhd_level_exchange_components": (C.c_int, [_P(Box), _P(C.c_void_p),
+                                                 _P(C.c_int64), C.c_int,
+                                                 C.c_int, C.c_char_p, C.c_int,
+                                                 _vp]),
     "grhd_checkpoint_write": (C.c_int, [C.c_char_p, _P(CheckpointHeader),
                                         C.c_char_p, _vp, C.c_int64, _P(Box),
                                         C.c_char_p, C.c_int, _vp]),

@@ -1733,8 +1733,21 @@ int grhd_level_exchange(const grhd_box *boxes, double *const *states,
                         const int64_t *strides, int count, char *err,
                         int err_cap, void *stream)
 {
+    return grhd_level_exchange_components(boxes, states, strides, count,
+                                          kStateComps, err, err_cap, stream);
+}
+
+int grhd_level_exchange_components(const grhd_box *boxes,
+                                   double *const *states,
+                                   const int64_t *strides, int count,
+                                   int ncomp, char *err, int err_cap,
+                                   void *stream)
+{
     if (count < 0 || (count > 0 && (!boxes || !states || !strides)))
         return io_error(err, err_cap, "null level arrays",
+                        GRHD_ERR_INVALID_ARG);
+    if (ncomp < 1 || ncomp > 256)
+        return io_error(err, err_cap, "component count out of range",
                         GRHD_ERR_INVALID_ARG);
     std::vector<BoxDev> b((size_t)count);
     for (int q = 0; q < count; ++q)
@@ -1785,7 +1798,7 @@ int grhd_level_exchange(const grhd_box *boxes, double *const *states,
             }
             if (any)
                 launch_copy_region(states[a], b[a], states[q], b[q], lo, hi,
-                                   s);
+                                   ncomp, s);
         }
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
@@ -1797,7 +1810,17 @@ int grhd_region_copy(int pack, double *state, int64_t state_cs,
                      const grhd_box *box, const int lo[3], const int hi[3],
                      double *buffer, void *stream)
 {
-    if (!state || !buffer || !lo || !hi || !valid_box(box))
+    return grhd_region_copy_components(pack, state, state_cs, box, lo, hi,
+                                       kStateComps, buffer, stream);
+}
+
+int grhd_region_copy_components(int pack, double *state, int64_t state_cs,
+                                const grhd_box *box, const int lo[3],
+                                const int hi[3], int ncomp, double *buffer,
+                                void *stream)
+{
+    if (!state || !buffer || !lo || !hi || !valid_box(box) || ncomp < 1 ||
+        ncomp > 256)
         return GRHD_ERR_INVALID_ARG;
     const BoxDev b = make_box(box, state_cs);
     if (state_cs < b.gvol())
@@ -1805,7 +1828,8 @@ int grhd_region_copy(int pack, double *state, int64_t state_cs,
     for (int d = 0; d < 3; ++d)
         if (lo[d] > hi[d] || lo[d] < b.glo[d] || hi[d] > b.ghi[d])
             return GRHD_ERR_INVALID_ARG;
-    launch_region(pack != 0, state, b, buffer, lo, hi, (cudaStream_t)stream);
+    launch_region(pack != 0, state, b, buffer, lo, hi, ncomp,
+                  (cudaStream_t)stream);
     return cudaGetLastError() == cudaSuccess ? GRHD_OK : GRHD_ERR_CUDA;
 }
 

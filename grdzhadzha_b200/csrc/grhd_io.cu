@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(256)
 __global__ void __launch_bounds__(256)
     k_copy_region(double *__restrict__ dst, BoxDev db,
                   const double *__restrict__ src, BoxDev sb, int lo0, int lo1,
-                  int lo2, int n0, int n1, int n2)
+                  int lo2, int n0, int n1, int n2, int ncomp)
 {
     const int64_t n = (int64_t)n0 * n1 * n2;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(256)
         const int j = lo1 + (int)(r % n1);
         const int k = lo2 + (int)(r / n1);
         const int64_t gd = db.gidx(i, j, k), gs = sb.gidx(i, j, k);
-        for (int c = 0; c < kStateComps; ++c)
+        for (int c = 0; c < ncomp; ++c)
             dst[c * db.cs + gd] = src[c * sb.cs + gs];
     }
 }
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(256)
 template <bool PACK>
 __global__ void __launch_bounds__(256)
     k_region(double *__restrict__ state, BoxDev b, double *__restrict__ buf,
-             int lo0, int lo1, int lo2, int n0, int n1, int n2)
+             int lo0, int lo1, int lo2, int n0, int n1, int n2, int ncomp)
 {
     const int64_t n = (int64_t)n0 * n1 * n2;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(256)
         const int j = lo1 + (int)(r % n1);
         const int k = lo2 + (int)(r / n1);
         const int64_t g = b.gidx(i, j, k);
-        for (int c = 0; c < kStateComps; ++c)
+        for (int c = 0; c < ncomp; ++c)
         {
             if (PACK)
                 buf[c * n + t] = state[c * b.cs + g];
@@ -197,26 +197,27 @@ void launch_checkpoint_to_state(const double *in, const BoxDev &b, int ncomp,
 
 void launch_copy_region(double *dst, const BoxDev &db, const double *src,
                         const BoxDev &sb, const int lo[3], const int hi[3],
-                        cudaStream_t s)
+                        int ncomp, cudaStream_t s)
 {
     const int n0 = hi[0] - lo[0] + 1, n1 = hi[1] - lo[1] + 1,
               n2 = hi[2] - lo[2] + 1;
     k_copy_region<<<grid_of((int64_t)n0 * n1 * n2), 256, 0, s>>>(
-        dst, db, src, sb, lo[0], lo[1], lo[2], n0, n1, n2);
+        dst, db, src, sb, lo[0], lo[1], lo[2], n0, n1, n2, ncomp);
 }
 
 void launch_region(bool pack, double *state, const BoxDev &b, double *buf,
-                   const int lo[3], const int hi[3], cudaStream_t s)
+                   const int lo[3], const int hi[3], int ncomp,
+                   cudaStream_t s)
 {
     const int n0 = hi[0] - lo[0] + 1, n1 = hi[1] - lo[1] + 1,
               n2 = hi[2] - lo[2] + 1;
     const int g = grid_of((int64_t)n0 * n1 * n2);
     if (pack)
         k_region<true><<<g, 256, 0, s>>>(state, b, buf, lo[0], lo[1], lo[2],
-                                         n0, n1, n2);
+                                         n0, n1, n2, ncomp);
     else
         k_region<false><<<g, 256, 0, s>>>(state, b, buf, lo[0], lo[1], lo[2],
-                                          n0, n1, n2);
+                                          n0, n1, n2, ncomp);
 }
 
 } // namespace grhd

@@ -32,16 +32,17 @@ void launch_state_to_checkpoint(const double *state, const BoxDev &b,
 void launch_checkpoint_to_state(const double *in, const BoxDev &b, int ncomp,
                                 double *state, cudaStream_t s);
 
-// LevelData::exchange between two boxes of a level: the 11 components of
-// the cells [lo, hi] (level index space) from `src` (box sb) to `dst`
-// (box db).
+// LevelData::exchange between two boxes of a level: the first `ncomp`
+// components of the cells [lo, hi] (level index space) from `src` (box sb)
+// to `dst` (box db).
 void launch_copy_region(double *dst, const BoxDev &db, const double *src,
                         const BoxDev &sb, const int lo[3], const int hi[3],
-                        cudaStream_t s);
+                        int ncomp, cudaStream_t s);
 
-// The 11 components of the region [lo, hi] (inside the ghosted box) into
-// (pack) or out of a packed buffer [component][k][j][i].
+// The first `ncomp` components of the region [lo, hi] (inside the ghosted
+// box) into (pack) or out of a packed buffer [component][k][j][i].
 void launch_region(bool pack, double *state, const BoxDev &b, double *buf,
-                   const int lo[3], const int hi[3], cudaStream_t s);
+                   const int lo[3], const int hi[3], int ncomp,
+                   cudaStream_t s);
 
 } // namespace grhd

@@ -111,9 +111,10 @@ class DeviceRegions:
 
     def _copy(self, pack, level: LevelBox, lo, hi, buf: torch.Tensor):
         b = level.c_box()
-        st = self._lib.grhd_region_copy(
+        st = self._lib.grhd_region_copy_components(
             int(pack), _ptr(level.state), level.comp_stride(), C.byref(b),
-            (C.c_int * 3)(*lo), (C.c_int * 3)(*hi), _ptr(buf), _stream())
+            (C.c_int * 3)(*lo), (C.c_int * 3)(*hi),
+            int(level.state.shape[0]), _ptr(buf), _stream())
         if st != L.GRHD_OK:
             raise L.InvalidArgument(st, None) \
                 if st == L.GRHD_ERR_INVALID_ARG else L.GRHDError(st, None)
@@ -196,24 +197,25 @@ class HaloExchange:
         self._bufs = None
         self._pending = None
 
-    def _buffers(self, device):
-        if self._bufs is None or self._bufs[0] != device:
+    def _buffers(self, device, ncomp=11):
+        if self._bufs is None or self._bufs[0] != (device, ncomp):
             def mk(plan):
-                return [torch.empty(11 * region_cells(lo, hi),
+                return [torch.empty(ncomp * region_cells(lo, hi),
                                     dtype=torch.float64, device=device)
                         for _, lo, hi in plan]
-            self._bufs = (device, mk(self.sends), mk(self.recvs))
+            self._bufs = ((device, ncomp), mk(self.sends), mk(self.recvs))
         return self._bufs[1], self._bufs[2]
 
-    @property
-    def bytes_per_exchange(self) -> int:
-        return 8 * 11 * sum(region_cells(lo, hi)
-                            for _, lo, hi in self.sends)
+    def bytes_per_exchange(self, ncomp=11) -> int:
+        """Bytes this rank sends per exchange of an ncomp-component state."""
+        return 8 * ncomp * sum(region_cells(lo, hi)
+                               for _, lo, hi in self.sends)
 
     def begin(self, level: LevelBox):
         if self._pending is not None:
             raise RuntimeError("exchange already in flight")
-        sbufs, rbufs = self._buffers(level.state.device)
+        sbufs, rbufs = self._buffers(level.state.device,
+                                     int(level.state.shape[0]))
         for (_, lo, hi), buf in zip(self.sends, sbufs):
             self.regions.pack(level, lo, hi, buf)
         self._pending = self.transport.start(
@@ -225,7 +227,8 @@ class HaloExchange:
             raise RuntimeError("no exchange in flight")
         self.transport.wait(self._pending)
         self._pending = None
-        _, rbufs = self._buffers(level.state.device)
+        _, rbufs = self._buffers(level.state.device,
+                                 int(level.state.shape[0]))
         for (_, lo, hi), buf in zip(self.recvs, rbufs):
             self.regions.unpack(level, lo, hi, buf)
 

@@ -158,15 +158,20 @@ class LevelBox:
 
 def level_exchange(boxes) -> None:
     """LevelData<FArrayBox>::exchange() over the LevelBoxes of one level
-    (grhd_level_exchange): ghost cells inside the problem domain take the
-    values of the box that owns them."""
+    (grhd_level_exchange_components): ghost cells inside the problem domain
+    take all components of the box that owns them (11 GRHD ones, or 36 for
+    the operator on CCZ4-stored geometry)."""
     lib = L.load()
     n = len(boxes)
     arr = (L.Box * n)(*[b.c_box() for b in boxes])
     ptrs = (C.c_void_p * n)(*[_ptr(b.state).value for b in boxes])
     strides = (C.c_int64 * n)(*[b.comp_stride() for b in boxes])
+    ncomp = {int(b.state.shape[0]) for b in boxes}
+    if len(ncomp) != 1:
+        raise ValueError("the boxes of a level hold the same components")
     err = C.create_string_buffer(256)
-    st = lib.grhd_level_exchange(arr, ptrs, strides, n, err, 256, _stream())
+    st = lib.grhd_level_exchange_components(arr, ptrs, strides, n,
+                                            ncomp.pop(), err, 256, _stream())
     if st != L.GRHD_OK:
         cls = L.InvalidArgument if st == L.GRHD_ERR_INVALID_ARG \
             else L.GRHDError

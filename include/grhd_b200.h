@@ -442,6 +442,14 @@ int grhd_disk_diagnostics(grhd_ctx *ctx, const double *state,
 int grhd_level_exchange(const grhd_box *boxes, double *const *states,
                         const int64_t *state_comp_strides, int count,
                         char *err, int err_cap, void *stream);
+/* The same for states of `ncomp` components (1..256), e.g. the
+ * GRHD_CCZ4_NUM_VARS of the operator on CCZ4-stored geometry, whose
+ * geometry the exchange must move as well. */
+int grhd_level_exchange_components(const grhd_box *boxes,
+                                   double *const *states,
+                                   const int64_t *state_comp_strides,
+                                   int count, int ncomp, char *err,
+                                   int err_cap, void *stream);
 
 /* ---- The operator on CCZ4-stored geometry ----
  * LevelDataFiniteVolumeOperator (Source/Matter/GRHD/FArrayBoxFiniteVolume.hpp:
@@ -498,6 +506,13 @@ int grhd_ccz4_advance_ssprk2(grhd_ctx *ctx, double *state,
 int grhd_region_copy(int pack, double *state, int64_t state_comp_stride,
                      const grhd_box *box, const int lo[3], const int hi[3],
                      double *buffer, void *stream);
+/* The same for states of `ncomp` components (1..256); the buffer holds
+ * ncomp x cells values. */
+int grhd_region_copy_components(int pack, double *state,
+                                int64_t state_comp_stride,
+                                const grhd_box *box, const int lo[3],
+                                const int hi[3], int ncomp, double *buffer,
+                                void *stream);
 
 /* The binary disk drivers' Keplerian disk (kitp_primitive +
  * fill_kitp_level_data, Main_GRHDLevelDataBinaryPNKITPDisk.cpp:398-555),
