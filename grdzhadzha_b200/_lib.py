@@ -242,6 +242,9 @@ SIGNATURES = {
                                              C.c_int, _P(Diagnostics), _vp]),
     "grhd_ccz4_compute_max_inverse_dt": (C.c_int, [_vp, _vp, C.c_int64,
                                                    _P(Box), _dp, _dp, _vp]),
+    "grhd_ccz4_ssprk2_stage": (C.c_int, [_vp, C.c_int, _vp, C.c_int64, _vp,
+                                         C.c_int64, _P(Box), _dp, C.c_double,
+                                         _P(Diagnostics), _vp]),
     "grhd_ccz4_advance_ssprk2": (C.c_int, [_vp, _vp, C.c_int64, _P(Box), _dp,
                                            C.c_double, _P(Diagnostics), _vp]),
     "grhd_default_kitp_disk_config": (None, [_P(KitpDiskConfig)]),

@@ -1091,6 +1091,59 @@ int grhd_ccz4_advance_ssprk2(grhd_ctx *ctx, double *state, int64_t state_cs,
     return st;
 }
 
+int grhd_ccz4_ssprk2_stage(grhd_ctx *ctx, int stage, double *state,
+                           int64_t state_cs, double *stage_state,
+                           int64_t stage_cs, const grhd_box *box,
+                           const double inverse_dx[3], double dt,
+                           grhd_diagnostics *diag, void *stream)
+{
+    if (ctx && (!inverse_dx || !stage_state || (stage != 1 && stage != 2)))
+    {
+        std::memset(&ctx->last_error, 0, sizeof(ctx->last_error));
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "ssprk2 stage is 1 or 2 and needs a stage state and "
+                         "inverse_dx");
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    BoxDev b;
+    int st = ccz4_checks(ctx, state, state_cs, box, -1, b, s);
+    if (st)
+        return st;
+    const BoxDev sb = make_box(box, stage_cs);
+    if ((st = check_strides(ctx, sb, stage_cs, -1)))
+        return st;
+    const int64_t gv = b.gvol();
+    if (stage == 1)
+    {
+        // stage = state (all components); rhs_initial = L(state); stage +=
+        // dt rhs_initial, recovered
+        GRHD_CUDA(ctx, cudaMemcpy2DAsync(stage_state, stage_cs * sizeof(double),
+                                         state, state_cs * sizeof(double),
+                                         gv * sizeof(double),
+                                         GRHD_CCZ4_NUM_VARS,
+                                         cudaMemcpyDeviceToDevice, s));
+        enqueue_ccz4_rhs(ctx, ctx->kbuf, b.ivol(), state, b, inverse_dx, s);
+        launch_ccz4_update(stage_state, nullptr, 0, ctx->kbuf, b.ivol(), sb,
+                           dt, 0, s);
+        launch_ccz4_recover(stage_state, sb, ctx->opt, ctx->status, s);
+    }
+    else
+    {
+        // rhs_stage = L(stage); state = (state + stage + dt rhs_stage) / 2,
+        // recovered
+        enqueue_ccz4_rhs(ctx, ctx->kbuf, b.ivol(), stage_state, sb,
+                         inverse_dx, s);
+        launch_ccz4_update(state, stage_state, stage_cs, ctx->kbuf, b.ivol(),
+                           b, dt, 1, s);
+        launch_ccz4_recover(state, b, ctx->opt, ctx->status, s);
+    }
+    ctx->launches += 2;
+    st = stage == 1 ? ccz4_finish(ctx, sb, stage_state, s)
+                    : ccz4_finish(ctx, b, state, s);
+    read_diag(ctx, diag);
+    return st;
+}
+
 int grhd_advance_ssprk2(grhd_ctx *ctx, double *state, int64_t state_cs,
                         const grhd_box *box, const double inverse_dx[3],
                         double time, double dt, grhd_diagnostics *diag,

@@ -752,6 +752,29 @@ class LevelDataFiniteVolumeOperator:
         m = self.compute_max_inverse_dt(state, domain_box, inverse_dx_U)
         return cfl / max(m, 1.0e-14)
 
+    def ssprk2_stage(self, stage, state: LevelBox, stage_state: LevelBox,
+                     dt, inverse_dx_U=None):
+        """One half of advance_ssprk2 for a level whose ghosts the caller
+        exchanges before each (grhd_ccz4_ssprk2_stage)."""
+        d = L.Diagnostics()
+        b = state.c_box()
+        self._check(self._lib.grhd_ccz4_ssprk2_stage(
+            self._ctx, int(stage), self._state(state), state.comp_stride(),
+            self._state(stage_state), stage_state.comp_stride(), C.byref(b),
+            self._inv(inverse_dx_U), dt, C.byref(d), _stream()))
+        return d
+
+    def advance_level_ssprk2(self, boxes, stage_boxes, dt, inverse_dx_U=None):
+        """advance_ssprk2 (:1323-1348) of a level of several boxes on this
+        device, LevelData::exchange() of all 36 components before each
+        RHS."""
+        level_exchange(boxes)
+        for b, sb in zip(boxes, stage_boxes):
+            self.ssprk2_stage(1, b, sb, dt, inverse_dx_U)
+        level_exchange(stage_boxes)
+        for b, sb in zip(boxes, stage_boxes):
+            self.ssprk2_stage(2, b, sb, dt, inverse_dx_U)
+
     def advance_ssprk2(self, state: LevelBox, domain=None, inverse_dx_U=None,
                        dt=None):
         d = L.Diagnostics()

@@ -492,6 +492,17 @@ int grhd_ccz4_compute_max_inverse_dt(grhd_ctx *ctx, const double *state,
                                      const grhd_box *box,
                                      const double inverse_dx[3], double *out,
                                      void *stream);
+/* advance_ssprk2 (:1323-1348) cut at its two RHS evaluations, for a level
+ * of several boxes or ranks whose ghosts (all 36 components) the caller
+ * exchanges before each stage, as grhd_ssprk2_stage for the fixed
+ * background: stage 1 copies the state into stage_state and adds dt L(state)
+ * (recovered); stage 2 sets state = (state + stage_state + dt
+ * L(stage_state)) / 2 (recovered). */
+int grhd_ccz4_ssprk2_stage(grhd_ctx *ctx, int stage, double *state,
+                           int64_t state_comp_stride, double *stage_state,
+                           int64_t stage_comp_stride, const grhd_box *box,
+                           const double inverse_dx[3], double dt,
+                           grhd_diagnostics *diag, void *stream);
 /* advance_ssprk2 (:1323-1348); the box must be the whole domain. */
 int grhd_ccz4_advance_ssprk2(grhd_ctx *ctx, double *state,
                              int64_t state_comp_stride, const grhd_box *box,
