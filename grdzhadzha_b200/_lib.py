@@ -248,6 +248,9 @@ SIGNATURES = {
     "grhd_ccz4_advance_ssprk2": (C.c_int, [_vp, _vp, C.c_int64, _P(Box), _dp,
                                            C.c_double, _P(Diagnostics), _vp]),
     "grhd_default_kitp_disk_config": (None, [_P(KitpDiskConfig)]),
+    "grhd_kitp_advance_ssprk2": (C.c_int, [_vp, _vp, C.c_int64, _P(Box), _dp,
+                                           _P(KitpConfig), C.c_double,
+                                           C.c_double, _P(Diagnostics), _vp]),
     "grhd_kitp_disk_initial_data": (C.c_int, [_vp, _vp, C.c_int64, _P(Box),
                                               _P(KitpDiskConfig), C.c_double,
                                               _vp]),

@@ -1641,6 +1641,58 @@ int grhd_kitp_sink_decay(grhd_ctx *ctx, double *state, int64_t state_cs,
     return GRHD_OK;
 }
 
+int grhd_kitp_advance_ssprk2(grhd_ctx *ctx, double *state, int64_t state_cs,
+                             const grhd_box *box, const double inverse_dx[3],
+                             const grhd_kitp_config *cfg, double time,
+                             double dt, grhd_diagnostics *diag, void *stream)
+{
+    if (ctx && ctx->params.precision != GRHD_PRECISION_FP64)
+    {
+        std::memset(&ctx->last_error, 0, sizeof(ctx->last_error));
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "the disk driver's step runs in FP64");
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    BoxDev b, bk;
+    KitpDev k0, k1, kh;
+    int st;
+    if ((st = kitp_setup(ctx, state, box, state_cs, cfg, time, bk, k0)) ||
+        (st = kitp_setup(ctx, state, box, state_cs, cfg, time + dt, bk, k1)) ||
+        (st = kitp_setup(ctx, state, box, state_cs, cfg, time + 0.5 * dt, bk,
+                         kh)) ||
+        (st = advance_checks(ctx, state, state_cs, box, inverse_dx, b, s)))
+        return st;
+    BoxDev sb = b;
+    sb.cs = b.gvol();
+    const Background bg0 = make_background(ctx->params, time);
+    const Background bg1 = make_background(ctx->params, time + dt);
+    double *k = ctx->kbuf;
+    const bool visc = cfg->alpha_viscosity != 0.0;
+    // advance_kitp_ssprk2 (Main_GRHDLevelDataBinaryPNKITPDisk.cpp:842-876):
+    // rhs = L(state) + viscous(state); stage = state + dt rhs, recovered at
+    // t + dt (its primitives kept: the viscous stress reads them);
+    // rhs = L(stage) + viscous(stage); state = (state + stage + dt rhs) / 2;
+    // sink decay at t + dt/2; recovery at t + dt
+    enqueue_rhs<double>(ctx, k, state, b, bg0, inverse_dx, s, false, 0.5 * dt);
+    if (visc)
+        launch_kitp_viscous_rhs(k, b.ivol(), state, b, ctx->opt, k0, s);
+    launch_stage<double>(1, state, b.cs, nullptr, 0, ctx->stage, sb.cs, k,
+                         nullptr, ctx->prim, ctx->src, 3, b, bg1, ctx->opt, 0,
+                         dt, false, inverse_dx, ctx->status, s);
+    enqueue_rhs<double>(ctx, k, ctx->stage, sb, bg1, inverse_dx, s, true,
+                        0.5 * dt);
+    if (visc)
+        launch_kitp_viscous_rhs(k, b.ivol(), ctx->stage, sb, ctx->opt, k1, s);
+    launch_kitp_combine(state, b, ctx->stage, sb.cs, k, b.ivol(), dt, s);
+    if (cfg->sink_rate != 0.0 && cfg->sink_size > 0.0)
+        launch_kitp_sink_decay(state, b, ctx->opt, kh, dt, s);
+    launch_recover(state, b, bg1, ctx->opt, ctx->status, s);
+    ctx->launches += 4 + (visc ? 2 : 0);
+    st = finish_status(ctx, b, state, bg0, s);
+    read_diag(ctx, diag);
+    return st;
+}
+
 } // extern "C"
 
 // ---------------------------------------------------------------------------

@@ -283,6 +283,25 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+__global__ void __launch_bounds__(256)
+    k_kitp_combine(double *__restrict__ s, BoxDev b,
+                   const double *__restrict__ u1, int64_t ucs,
+                   const double *__restrict__ k, int64_t rcs, double dt)
+{
+    const int64_t n = b.ivol();
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x)
+    {
+        int i, j, l;
+        cell_of_interior(b, t, i, j, l);
+        const int64_t g = b.gidx(i, j, l);
+        // RHS components D, S1..3, tau are the state's first five
+        for (int c = 0; c < 5; ++c)
+            s[c * b.cs + g] =
+                0.5 * (s[c * b.cs + g] + u1[c * ucs + g] + dt * k[c * rcs + t]);
+    }
+}
+
 int blocks_for(int64_t n)
 {
     int64_t g = (n + 255) / 256;
@@ -321,6 +340,14 @@ void launch_kitp_disk_fill(double *state, const BoxDev &b,
                            const KitpDiskDev &k, cudaStream_t s)
 {
     k_kitp_disk_fill<<<blocks_for(b.gvol()), 256, 0, s>>>(state, b, bg, o, k);
+}
+
+void launch_kitp_combine(double *state, const BoxDev &b, const double *u1,
+                         int64_t u1_cs, const double *k, int64_t rcs,
+                         double dt, cudaStream_t s)
+{
+    k_kitp_combine<<<blocks_for(b.ivol()), 256, 0, s>>>(state, b, u1, u1_cs, k,
+                                                        rcs, dt);
 }
 
 } // namespace grhd

@@ -33,6 +33,14 @@ void launch_kitp_sink_rhs(double *rhs, int64_t rcs, const double *state,
 void launch_kitp_sink_decay(double *state, const BoxDev &b, const Options &o,
                             const KitpDev &k, double dt, cudaStream_t s);
 
+// combine_ssprk2_conserved_state (FArrayBoxFiniteVolume.hpp:942-969) on the
+// interior conserved variables, without a recovery: s = (s + u1 + dt k) / 2
+// (the disk driver decays its sinks between the combination and the
+// recovery, advance_kitp_ssprk2 :842-876).
+void launch_kitp_combine(double *state, const BoxDev &b, const double *u1,
+                         int64_t u1_cs, const double *k, int64_t rcs,
+                         double dt, cudaStream_t s);
+
 // The disk drivers' Keplerian disk (kitp_primitive, :398-520) with the
 // azimuthal density modes m = 1..4 (new): the binary (masses, separation,
 // softening, orbital frequency, body positions at the fill time) and the

@@ -499,6 +499,19 @@ class _OperatorBase:
             self._ctx, _ptr(rhs), rhs[0].numel(), _ptr(state.state),
             state.comp_stride(), C.byref(b), C.byref(cfg), time, _stream()))
 
+    def kitp_advance_ssprk2(self, state: LevelBox, time, dt, config=None,
+                            inverse_dx_U=None):
+        """advance_kitp_ssprk2 (Main_GRHDLevelDataBinaryPNKITPDisk.cpp:
+        842-876), the disk driver's step (grhd_kitp_advance_ssprk2)."""
+        cfg = config if config is not None else kitp_config()
+        d = L.Diagnostics()
+        b = state.c_box()
+        self._check(self._lib.grhd_kitp_advance_ssprk2(
+            self._ctx, _ptr(state.state), state.comp_stride(), C.byref(b),
+            self._inv(inverse_dx_U), C.byref(cfg), time, dt, C.byref(d),
+            _stream()))
+        return d
+
     def kitp_sink_decay(self, state: LevelBox, time, dt, config=None):
         """apply_kitp_sink_decay (:612-662) with the bodies at `time`."""
         cfg = config if config is not None else kitp_config()

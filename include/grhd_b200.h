@@ -419,6 +419,18 @@ int grhd_kitp_sink_decay(grhd_ctx *ctx, double *state,
                          const grhd_kitp_config *config, double time,
                          double dt, void *stream);
 
+/* advance_kitp_ssprk2 (:842-876), the disk driver's step, on one box
+ * covering the domain: SSPRK2 whose RHS is the operator's plus the viscous
+ * stress divergence (the sink term enters as the decay, not the RHS), the
+ * stage recovered at time + dt, the combination, the sink decay at
+ * time + dt/2, the recovery at time + dt.  FP64; needs the binary PN
+ * background.  `diag` (may be NULL) accumulates both recoveries. */
+int grhd_kitp_advance_ssprk2(grhd_ctx *ctx, double *state,
+                             int64_t state_comp_stride, const grhd_box *box,
+                             const double inverse_dx[3],
+                             const grhd_kitp_config *config, double time,
+                             double dt, grhd_diagnostics *diag, void *stream);
+
 /* ---- example drivers' diagnostics and checkpoints ---- */
 
 /* compute_diagnostics of the example drivers
