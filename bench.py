@@ -608,6 +608,19 @@ def run_widened(hbm_peak):
         ms = _time(fn, reps=5)
         out[name] = {"value": lv.num_cells / (ms / 1e3),
                      "unit": "cells/s", "ms": ms}
+    # the disk driver's step (operator RHS + viscous stress, sink decay)
+    dt = 0.5 * op.compute_stable_dt(lv, cfl=CFL)
+    st = {"t": 0.0}
+
+    def kitp_step():
+        op.kitp_advance_ssprk2(lv, st["t"], dt, cfg)
+        st["t"] += dt
+    from grdzhadzha_b200.operator import kitp_config
+    cfg = kitp_config()
+    ms = _time(kitp_step, reps=3, warmup=1)
+    out["kitp_ssprk2_step_128"] = {
+        "value": lv.num_cells / (ms / 1e3), "unit": "cell-updates/s",
+        "ms": ms, "note": "SSPRK2 step, FP64, viscosity and sinks on"}
     torch.cuda.empty_cache()
     return out
 
