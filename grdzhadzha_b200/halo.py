@@ -243,7 +243,10 @@ class DistributedLevel:
 
     op: a FixedBG / TimeDependentFixedBG operator; boxes: the level's
     boxes (the same list on every rank, e.g. slab_boxes); transport:
-    TorchTransport (default) or LocalTransport."""
+    TorchTransport (default) or LocalTransport.  For the operator on
+    CCZ4-stored geometry, drive a HaloExchange over its 36-component
+    LevelBoxes and its ssprk2_stage directly (the exchange moves every
+    component the state holds)."""
 
     def __init__(self, op, boxes, rank, domain_lo, domain_hi,
                  transport=None, device="cuda", regions=None):
