@@ -169,6 +169,7 @@ SIGNATURES = {
     "grhd_compute_rhs_static": (C.c_int, [_vp, _vp, C.c_int64, _vp,
                                           C.c_int64, _P(Box), _dp,
                                           C.c_double, _vp]),
+    "grhd_static_scratch_fill": (C.c_int, [_vp, C.c_double, _vp]),
     "grhd_recover_primitives": (C.c_int, [_vp, _vp, C.c_int64, _P(Box),
                                           C.c_double, _P(Diagnostics), _vp]),
     "grhd_update_conserved": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_int64,

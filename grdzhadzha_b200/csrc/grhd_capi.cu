@@ -2201,6 +2201,16 @@ int static_scratch(grhd_ctx *ctx, double **out)
     return GRHD_OK;
 }
 
+__global__ void k_static_scratch_fill(double v)
+{
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+         q < kStaticDoubles; q += (int64_t)gridDim.x * blockDim.x)
+        g_rhs_scratch[q] = v;
+}
+
+// The three RHS launches count in the context's launch counter; they are
+// not timed by the per-kernel profile (that would take events from the
+// context's pool).
 template <typename T>
 void enqueue_rhs_static(grhd_ctx *ctx, T *rhs, double *state, const BoxDev &b,
                         const Background &bg, const double inv_dx[3],
@@ -2240,8 +2250,7 @@ extern "C" int grhd_compute_rhs_static(grhd_ctx *ctx, double *rhs,
     const BoxDev b = make_box(box, state_cs);
     if ((st = check_strides(ctx, b, state_cs, rhs_cs)))
         return st;
-    if (b.gvol() > kStaticGhostedCells || b.ivol() > kStaticInteriorCells ||
-        face_kernel_blocks(b, ctx->zchunk) > kStaticMdotBlocks)
+    if (b.gvol() > kStaticGhostedCells || b.ivol() > kStaticInteriorCells)
     {
         char msg[200];
         std::snprintf(msg, sizeof(msg),
@@ -2250,6 +2259,17 @@ extern "C" int grhd_compute_rhs_static(grhd_ctx *ctx, double *rhs,
                       (long long)b.gvol(), (long long)b.ivol(),
                       (long long)kStaticGhostedCells,
                       (long long)kStaticInteriorCells);
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, nullptr,
+                         0.0, msg);
+    }
+    if (face_kernel_blocks(b, ctx->zchunk) > kStaticMdotBlocks)
+    {
+        char msg[200];
+        std::snprintf(msg, sizeof(msg),
+                      "box too large for the static RHS scratch: its face "
+                      "pass needs %lld accretion partials (limit %lld)",
+                      (long long)face_kernel_blocks(b, ctx->zchunk),
+                      (long long)kStaticMdotBlocks);
         return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, nullptr,
                          0.0, msg);
     }
@@ -2279,6 +2299,22 @@ extern "C" int grhd_compute_rhs_static(grhd_ctx *ctx, double *rhs,
                                            cudaMemcpyDeviceToDevice, s));
     }
     return finish_status(ctx, b, state, bg, s);
+}
+
+// Test support: sets every word of the fixed array on the context's device
+// to `value`, so that a test can show that no word of it has to hold any
+// particular value before a grhd_compute_rhs_static call.
+extern "C" int grhd_static_scratch_fill(grhd_ctx *ctx, double value,
+                                        void *stream)
+{
+    if (!ctx)
+        return GRHD_ERR_INVALID_ARG;
+    GRHD_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    k_static_scratch_fill<<<148, 256, 0, s>>>(value);
+    GRHD_CUDA(ctx, cudaGetLastError());
+    GRHD_CUDA(ctx, cudaStreamSynchronize(s));
+    return GRHD_OK;
 }
 
 // Host helpers shared with the ensemble driver (grhd_ensemble.cu).

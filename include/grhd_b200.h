@@ -129,7 +129,9 @@ typedef struct grhd_box
     int domain_lo[3], domain_hi[3];
 } grhd_box;
 
-/* AtmosphereResetDiagnostics, FArrayBoxFiniteVolume.hpp:78-92 */
+/* AtmosphereResetDiagnostics, FArrayBoxFiniteVolume.hpp:78-92.  Every entry
+ * point that takes a `diag` adds its counts to it (as the reference's
+ * operator += does, :104-110): zero it before the first call. */
 typedef struct grhd_diagnostics
 {
     long long num_cells, num_failed_recoveries, num_floored_primitives,
@@ -174,15 +176,26 @@ int grhd_compute_rhs(grhd_ctx *ctx, double *rhs, int64_t rhs_comp_stride,
  * Limits: at most 65536 ghosted and 32768 interior cells (e.g. a 32^3 box
  * with 2 ghosts); larger boxes return GRHD_ERR_INVALID_ARG.  The first
  * call on each device looks the array up (cudaGetSymbolAddress with that
- * device current) and caches its address: make one call per device
- * before any stream capture begins.  All calls on a device share the
+ * device current) and caches its address for the life of the process:
+ * make that first call before any stream capture begins on the device,
+ * and make no call after a reset of the device (cudaDeviceReset), which
+ * leaves the cached address stale.  All calls on a device share the
  * array, so calls that overlap in time there (other streams, threads or
- * contexts) race: issue them one after another. */
+ * contexts) race: issue them one after another.  Like grhd_compute_rhs,
+ * the call synchronizes `stream` to read the status word.  Its kernels
+ * count in the context's launch counter but not in the per-kernel
+ * profile (grhd_profile_read). */
 int grhd_compute_rhs_static(grhd_ctx *ctx, double *rhs,
                             int64_t rhs_comp_stride, double *state,
                             int64_t state_comp_stride, const grhd_box *box,
                             const double inverse_dx[3], double time,
                             void *stream);
+
+/* Test support for grhd_compute_rhs_static (no counterpart in the
+ * reference): sets every word of its fixed array on the context's device
+ * to `value` and synchronizes `stream`.  Lets a test show that the RHS
+ * does not depend on what earlier calls left in the array. */
+int grhd_static_scratch_fill(grhd_ctx *ctx, double value, void *stream);
 
 /* recover_primitives(state[, time]) -> AtmosphereResetDiagnostics,
  * :506-520 / :728-743.  `diag` may be NULL. */
