@@ -420,18 +420,28 @@ def run_adjoint(n, steps, every, fd_steps, hbm_peak):
 
 
 class CpuBaseline:
-    """The oracle (the reference's algorithm, per-box structure, one z-slab
-    box per host thread) on the same workload: a mid-plane z-slab of the
-    256^3 grid, nz = min(256, 16 x threads) planes, so each box is at
-    least 16 planes thick.  Its state is built by the oracle itself (torus
-    + numpy-seeded 1e-3 perturbation + recovery)."""
+    """The reference's algorithm on the host cores: the oracle's timing
+    build (oracle/liborc_grhd_fast.so, -O3 with AVX2 + FMA; the parity
+    checker is the no-contraction build of the same source) on a bounded
+    sample of the same workload -- the central 128 x 128 columns of the
+    256^3 torus grid over nz = min(256, 16 x threads) mid-plane z planes,
+    as one box whose RHS runs as z-slab boxes of at least 16 planes, one
+    thread each (the reference's per-box loops, its MPI ranks standing as
+    threads).  One sample is one complete step as the GPU arm's: the CFL
+    bound of the current state, then one RK4 step (4 RHS evaluations, the
+    stage combinations, the post-stage recoveries).  The sample's state is
+    built by the oracle (torus + numpy-seeded 1e-3 perturbation +
+    recovery)."""
+
+    BUILD = "gcc -O3 -march=x86-64-v3 -ffp-contract=fast"
 
     def __init__(self, threads):
+        import ctypes as C
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import numpy as np
         import oracle_lib as O
 
-        self.O = O
+        self.O, self.C = O, C
         self.threads = threads
         O.set_threads(threads)
         n = N_CELLS
@@ -445,15 +455,17 @@ class CpuBaseline:
                              rec_max_iterations=80,
                              rec_max_velocity_squared=0.9, limiter_theta=2.0,
                              excision_radius=1.5)
+        nxy = 128
         nz = min(n, 16 * threads)
         box = O.Box()
-        z0 = n // 2 - nz // 2
-        for d, (lo, hi) in enumerate(((0, n - 1), (0, n - 1),
+        x0, z0 = n // 2 - nxy // 2, n // 2 - nz // 2
+        for d, (lo, hi) in enumerate(((x0, x0 + nxy - 1),
+                                      (x0, x0 + nxy - 1),
                                       (z0, z0 + nz - 1))):
             box.lo[d], box.hi[d] = lo, hi
             box.glo[d], box.ghi[d] = lo - 2, hi + 2
             box.dlo[d], box.dhi[d] = 0, n - 1
-        box.comp_stride = (n + 4) * (n + 4) * (nz + 4)
+        box.comp_stride = (nxy + 4) * (nxy + 4) * (nz + 4)
         s = O.new_state(box)
         cfg = O.torus_config(total_mass=1.0, inner_radius=6.0,
                              pressure_max_radius=12.0, rho_peak=1.0,
@@ -466,20 +478,41 @@ class CpuBaseline:
         V[O.EPS] = V[O.PRESS] / ((GAMMA - 1.0) * V[O.RHO])
         O.fill_conserved_from_primitives(p, box, s)
         O.recover_primitives(p, box, s)
-        self.p, self.box, self.s, self.nz = p, box, s, nz
-        self.cells = n * n * nz
-        self.desc = (f"one RHS evaluation of the oracle (the reference's "
-                     f"per-box algorithm, {threads} z-slab boxes of "
+        O.set_threads(1)
+        self.L = O.fast_lib()
+        self.L.orc_set_threads(threads)
+        self.p, self.box, self.s = p, box, s
+        self.inv = np.array([1.0 / dx] * 3)
+        self.t = 0.0
+        self.cells = nxy * nxy * nz
+        self.desc = (f"one RK4 step with its CFL bound (4 RHS evaluations, "
+                     f"stage combinations, post-stage recoveries) of the "
+                     f"oracle's timing build ({self.BUILD}; the reference's "
+                     f"per-box algorithm, z-slab boxes of "
                      f"{nz // threads}+ planes, one thread each) over the "
-                     f"{n}x{n}x{nz} mid-plane slab of the {n}^3 grid; "
-                     f"RK4 step = 4 RHS evaluations")
+                     f"central {nxy}x{nxy}x{nz} cells of the {n}^3 grid")
 
     def sample(self):
-        """RK4-equivalent cell-updates/s of one RHS evaluation."""
+        """(cell-updates/s, seconds) of one step of the sample."""
+        O, C, L = self.O, self.C, self.L
+        err = O.Error()
+        diag = O.Diag()
+        mi = C.c_double()
         t0 = time.perf_counter()
-        self.O.compute_rhs_slabs(self.p, self.box, self.s, self.threads)
+        st = L.orc_compute_max_inverse_dt(C.byref(self.p), C.byref(self.box),
+                                          O._dp(self.s), O._dp(self.inv),
+                                          self.t, C.byref(mi), C.byref(err))
+        if st:
+            raise RuntimeError(f"oracle CFL bound failed ({st})")
+        dt = CFL / max(mi.value, 1e-14)
+        st = L.orc_advance_rk4(C.byref(self.p), C.byref(self.box),
+                               O._dp(self.s), O._dp(self.inv), self.t, dt,
+                               C.byref(diag), C.byref(err))
         el = time.perf_counter() - t0
-        return self.cells / el / 4.0
+        if st:
+            raise RuntimeError(f"oracle RK4 step failed ({st})")
+        self.t += dt
+        return self.cells / el, el
 
 
 # ------------------------------------------- widened rows (one GPU each)
@@ -671,24 +704,24 @@ def main():
             return
         threads = host_threads()
         cb = CpuBaseline(threads)
-        samples = []
-        for i in range(args.warmup + args.steps):
-            rate = cb.sample()
-            if i >= args.warmup:
-                samples.append(rate)
-        value = statistics.median(samples)
-        sample_desc = cb.desc
+        for _ in range(args.warmup):
+            cb.sample()
+        secs = [cb.sample()[1] for _ in range(args.steps)]
+        total = sum(secs)
+        value = cb.cells * args.steps / total
         line = {
             "impl": "reference", "metric": METRIC, "value": value,
             "unit": "cell-updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": N_CELLS ** 3 / value * 1e3,
+            "ms_per_step": total / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
             "config": workload_config(N_CELLS),
             "cpu_baseline": {"value": value, "unit": "cell-updates/s",
                              "cores": threads, "kind": "port",
-                             "sample": sample_desc},
+                             "build": CpuBaseline.BUILD,
+                             "sample": cb.desc,
+                             "cells_per_step": cb.cells},
             "e2e": {"value": value, "unit": "cell-updates/s",
                     "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
@@ -765,9 +798,11 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = host_threads()
         cb = CpuBaseline(threads)
-        rate = max(cb.sample() for _ in range(2))
+        cb.sample()
+        rate = max(cb.sample()[0] for _ in range(2))
         cpu = {"value": rate, "unit": "cell-updates/s", "cores": threads,
-               "kind": "port", "sample": cb.desc}
+               "kind": "port", "build": CpuBaseline.BUILD,
+               "sample": cb.desc, "cells_per_step": cb.cells}
     if rank == 0:
         line = {
             "metric": METRIC, "value": res["value"],
@@ -786,6 +821,30 @@ def main():
             "gpu_launches": res["launches"], "kernel_ms": res["kernel_ms"],
         }
         if variants is not None:
+            # the headline variants as top-level keys, ahead of the long
+            # `variants` object
+            mx = variants.get("mixed")
+            if mx:
+                line["mixed_value"] = mx["value"]
+                line["mixed_speedup_vs_fp64"] = mx["speedup_vs_fp64"]
+            ens = variants.get("batched_ensemble", {})
+            if "fp64" in ens:
+                line["batched_fp64_value"] = ens["fp64"]["value"]
+            if "mixed" in ens:
+                line["batched_mixed_value"] = ens["mixed"]["value"]
+                line["batched_mixed_speedup_vs_fp64_plain"] = (
+                    ens["mixed"]["speedup_vs_fp64_plain"])
+            adj = variants.get("adjoint")
+            if adj:
+                line["adjoint_backward_over_forward"] = (
+                    adj["backward_over_forward"])
+                rows = adj.get("fd_check", {}).get("rows", {})
+                if rows:
+                    line["adjoint_fd_max_rel_err"] = max(
+                        r["rel_err"][0] for r in rows.values())
+                if "tlm_check" in adj:
+                    line["adjoint_tlm_max_rel_err"] = max(
+                        c["rel_err"] for c in adj["tlm_check"])
             line["variants"] = variants
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -1,6 +1,11 @@
-"""In-tree build of libgrhd_b200.so for sm_100a (nvcc, no JIT cache)."""
+"""In-tree build of libgrhd_b200.so for sm_100a (nvcc, no JIT cache).
+
+Each CUDA source compiles to its own object under grdzhadzha_b200/_build/
+(in parallel; an object is rebuilt when its source or any header is newer),
+then nvcc links the shared library."""
 from __future__ import annotations
 
+import concurrent.futures as cf
 import os
 import subprocess
 import sys
@@ -8,16 +13,15 @@ import sys
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _ROOT = os.path.dirname(_HERE)
 CSRC = os.path.join(_HERE, "csrc")
+BUILD_DIR = os.path.join(_HERE, "_build")
 SOURCES = ["grhd_kernels.cu", "grhd_initial_data.cu", "grhd_capi.cu",
            "grhd_ensemble.cu", "grhd_adjoint.cu", "grhd_kitp.cu",
            "grhd_io.cu"]
 OUTPUT = os.path.join(_HERE, "libgrhd_b200.so")
 
-NVCC_FLAGS = [
-    "-gencode", "arch=compute_100a,code=sm_100a",
-    "-O3", "-std=c++17", "-lineinfo",
-    "-Xcompiler", "-fPIC", "-shared",
-]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo",
+                     "-Xcompiler", "-fPIC"]
 
 
 def nvcc() -> str:
@@ -27,21 +31,50 @@ def nvcc() -> str:
     return "nvcc"
 
 
-def needs_rebuild() -> bool:
-    if not os.path.exists(OUTPUT):
+def _headers():
+    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC)
+          if f.endswith((".cuh", ".h"))]
+    hs.append(os.path.join(_ROOT, "include", "grhd_b200.h"))
+    return hs
+
+
+def _obj(src: str) -> str:
+    return os.path.join(BUILD_DIR, src[:-3] + ".o")
+
+
+def _stale(target: str, deps) -> bool:
+    if not os.path.exists(target):
         return True
-    t = os.path.getmtime(OUTPUT)
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
-    deps.append(os.path.join(_ROOT, "include", "grhd_b200.h"))
+    t = os.path.getmtime(target)
     return any(os.path.getmtime(d) > t for d in deps)
+
+
+def needs_rebuild() -> bool:
+    deps = [os.path.join(CSRC, s) for s in SOURCES] + _headers()
+    return _stale(OUTPUT, deps)
+
+
+def _compile(src: str, verbose: bool) -> None:
+    cmd = [nvcc()] + NVCC_FLAGS + [
+        "-I", os.path.join(_ROOT, "include"), "-I", CSRC,
+        "-c", os.path.join(CSRC, src), "-o", _obj(src)]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_rebuild():
         return OUTPUT
-    cmd = [nvcc()] + NVCC_FLAGS + [
-        "-I", os.path.join(_ROOT, "include"), "-I", CSRC,
-        "-o", OUTPUT] + [os.path.join(CSRC, s) for s in SOURCES]
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    hs = _headers()
+    todo = [s for s in SOURCES
+            if force or _stale(_obj(s), [os.path.join(CSRC, s)] + hs)]
+    with cf.ThreadPoolExecutor(max_workers=max(1, len(todo))) as ex:
+        for f in [ex.submit(_compile, s, verbose) for s in todo]:
+            f.result()
+    cmd = [nvcc()] + ARCH + ["-shared", "-o", OUTPUT] + [
+        _obj(s) for s in SOURCES]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

@@ -1499,30 +1499,46 @@ static void recover_range(const orc_params *o, const orc_box *b,
 }
 
 /* compute_max_inverse_dt_from_fixed_background, :364-412 */
-int orc_compute_max_inverse_dt(const orc_params *o, const orc_box *b,
-                               const double *state, const double inv_dx[3],
-                               double t, double *out, orc_error *err)
+/* compute_max_inverse_dt of a box (:364-444), over the z planes k0..k1. */
+typedef struct
 {
-    if (err)
-        memset(err, 0, sizeof(*err));
+    const orc_params *o;
+    const orc_box *b;
+    const double *state;
+    const double *inv_dx;
+    double t;
+    double mx[256];
+    int status[256];
+    orc_error err[256];
+} CflJob;
+
+static void cfl_job(void *ctx, int k0, int k1, int slot)
+{
+    CflJob *c = (CflJob *)ctx;
+    const orc_params *o = c->o;
+    const orc_box *b = c->b;
     double mx = 0.0;
-    for (int k = b->lo[2]; k <= b->hi[2]; ++k)
+    c->status[slot] = ORC_OK;
+    memset(&c->err[slot], 0, sizeof(orc_error));
+    for (int k = k0; k <= k1; ++k)
         for (int j = b->lo[1]; j <= b->hi[1]; ++j)
             for (int i = b->lo[0]; i <= b->hi[0]; ++i)
             {
                 if (is_excised(o, i, j, k))
                     continue;
                 Geom g;
-                load_geometry(o, t, i, j, k, &g);
-                const Cons c = load_cons(b, state, fab_index(b, i, j, k));
+                load_geometry(o, c->t, i, j, k, &g);
+                const Cons cs = load_cons(b, c->state, fab_index(b, i, j, k));
                 Prim pr;
                 int it;
                 double res;
-                if (!con2prim(o, &c, g.gUU, &pr, &it, &res))
+                if (!con2prim(o, &cs, g.gUU, &pr, &it, &res))
                 {
-                    set_error(err, ORC_ERR_RECOVERY, ORC_WHERE_CFL, i, j, k,
-                              res);
-                    return ORC_ERR_RECOVERY;
+                    set_error(&c->err[slot], ORC_ERR_RECOVERY, ORC_WHERE_CFL,
+                              i, j, k, res);
+                    c->status[slot] = ORC_ERR_RECOVERY;
+                    c->mx[slot] = mx;
+                    return;
                 }
                 enforce_floors(o, &pr, g.gLL);
                 if (is_atmosphere(o, &pr, 1.0 + 1.0e-12))
@@ -1533,10 +1549,45 @@ int orc_compute_max_inverse_dt(const orc_params *o, const orc_box *b,
                     double lo, hi;
                     char_speeds(o->gamma, &pr, g.gLL, g.gUU, d, g.lapse,
                                 g.shift, &lo, &hi);
-                    cell += dmax(fabs(lo), fabs(hi)) * inv_dx[d];
+                    cell += dmax(fabs(lo), fabs(hi)) * c->inv_dx[d];
                 }
                 mx = dmax(mx, cell);
             }
+    c->mx[slot] = mx;
+}
+
+/* The maximum is exact, so splitting the planes over threads changes no
+ * result; the error reported is the first failing cell in the box's
+ * iteration order (the lowest failing slot's first failure). */
+int orc_compute_max_inverse_dt(const orc_params *o, const orc_box *b,
+                               const double *state, const double inv_dx[3],
+                               double t, double *out, orc_error *err)
+{
+    if (err)
+        memset(err, 0, sizeof(*err));
+    CflJob *c = (CflJob *)calloc(1, sizeof(CflJob));
+    c->o = o;
+    c->b = b;
+    c->state = state;
+    c->inv_dx = inv_dx;
+    c->t = t;
+    const int n = parallel_z(b->lo[2], b->hi[2], cfl_job, c, 256);
+    double mx = 0.0;
+    int status = ORC_OK;
+    for (int s = 0; s < n; ++s)
+    {
+        if (c->status[s] != ORC_OK)
+        {
+            status = c->status[s];
+            if (err)
+                *err = c->err[s];
+            break;
+        }
+        mx = dmax(mx, c->mx[s]);
+    }
+    free(c);
+    if (status != ORC_OK)
+        return status;
     *out = mx;
     return ORC_OK;
 }
@@ -1599,6 +1650,27 @@ static size_t box_interior_cells(const orc_box *b)
            (b->hi[2] - b->lo[2] + 1);
 }
 
+/* The RHS of an integrator stage: the single reference box, or -- when
+ * several threads are set and no accretion integral is wanted -- the same
+ * box cut into z-slab boxes, one thread each (orc_compute_rhs_slabs).  The
+ * two give the same RHS bit for bit: the slabs fill the level's physical
+ * ghosts with the single box's values, and every cell's faces and sources
+ * read the same neighbours. */
+static int stage_rhs(const orc_params *o, const orc_box *b, double *state,
+                     double *rhs, int64_t nr, const double inv_dx[3],
+                     double t, double *mdot, orc_error *err)
+{
+    if (g_threads > 1 && mdot == NULL)
+        return orc_compute_rhs_slabs(o, b, state, rhs, nr, inv_dx, t,
+                                     g_threads, err);
+    double m = 0.0;
+    const int st = orc_compute_rhs_mdot(o, b, state, rhs, nr, inv_dx, t, &m,
+                                        err);
+    if (mdot)
+        *mdot = m;
+    return st;
+}
+
 /* advance_ssprk2 of the time-dependent operator, :782-809 (the static
  * operator, :563-589, is the same with time ignored by the background). */
 int orc_advance_ssprk2(const orc_params *o, const orc_box *b, double *state,
@@ -1625,12 +1697,13 @@ int orc_advance_ssprk2_mdot(const orc_params *o, const orc_box *b,
     memcpy(old_state, state, ns * sizeof(double));
     memcpy(stage, state, ns * sizeof(double));
     double m0 = 0.0, m1 = 0.0;
-    int st = orc_compute_rhs_mdot(o, b, state, r0, nr, inv_dx, t, &m0, err);
+    int st = stage_rhs(o, b, state, r0, nr, inv_dx, t,
+                       mdot_integral ? &m0 : NULL, err);
     if (st == ORC_OK)
     {
         orc_update_conserved(o, b, stage, r0, nr, dt, t + dt, 1, diag);
-        st = orc_compute_rhs_mdot(o, b, stage, r1, nr, inv_dx, t + dt, &m1,
-                                  err);
+        st = stage_rhs(o, b, stage, r1, nr, inv_dx, t + dt,
+                       mdot_integral ? &m1 : NULL, err);
     }
     if (mdot_integral)
         *mdot_integral += 0.5 * dt * m0 + 0.5 * dt * m1;
@@ -1695,8 +1768,8 @@ int orc_advance_rk4_mdot(const orc_params *o, const orc_box *b, double *state,
     for (int s = 0; s < 4 && st == ORC_OK; ++s)
     {
         double ms = 0.0;
-        st = orc_compute_rhs_mdot(o, b, s == 0 ? state : stage, k, nr, inv_dx,
-                                  t_stage[s], &ms, err);
+        st = stage_rhs(o, b, s == 0 ? state : stage, k, nr, inv_dx,
+                       t_stage[s], mdot_integral ? &ms : NULL, err);
         if (st != ORC_OK)
             break;
         if (mdot_integral)
@@ -2393,10 +2466,23 @@ int orc_michel_point(const orc_params *p, const orc_michel_config *c,
 }
 
 /* fill_michel_state, GRHDLevelDataMichelAccretion.cpp:331-372 (ghosted) */
-int orc_fill_michel(const orc_params *p, const orc_michel_config *c,
-                    const orc_box *b, double *state)
+typedef struct
 {
-    for (int k = b->glo[2]; k <= b->ghi[2]; ++k)
+    const orc_params *p;
+    const orc_michel_config *c;
+    const orc_box *b;
+    double *state;
+    int status[256];
+} MichelFill;
+
+static void michel_fill_job(void *ctx, int k0, int k1, int slot)
+{
+    MichelFill *f = (MichelFill *)ctx;
+    const orc_params *p = f->p;
+    const orc_michel_config *c = f->c;
+    const orc_box *b = f->b;
+    f->status[slot] = ORC_OK;
+    for (int k = k0; k <= k1; ++k)
         for (int j = b->glo[1]; j <= b->ghi[1]; ++j)
             for (int i = b->glo[0]; i <= b->ghi[0]; ++i)
             {
@@ -2413,7 +2499,10 @@ int orc_fill_michel(const orc_params *p, const orc_michel_config *c,
                 {
                     double pt[5];
                     if (orc_michel_point(p, c, radius, pt) != ORC_OK)
-                        return ORC_ERR_SETUP;
+                    {
+                        f->status[slot] = ORC_ERR_SETUP;
+                        return;
+                    }
                     pr.rho = pt[0];
                     pr.eps = pt[2];
                     pr.p = pt[1];
@@ -2422,11 +2511,29 @@ int orc_fill_michel(const orc_params *p, const orc_michel_config *c,
                     enforce_floors(p, &pr, g.gLL);
                 }
                 const int64_t idx = fab_index(b, i, j, k);
-                store_prim(b, state, idx, &pr);
+                store_prim(b, f->state, idx, &pr);
                 const Cons cc = p2c(p->gamma, &pr, g.gLL);
-                store_cons(b, state, idx, &cc);
+                store_cons(b, f->state, idx, &cc);
             }
-    return ORC_OK;
+}
+
+/* fill_michel_state (Tests/GRHDLevelDataMichelAccretion/...cpp:312-372)
+ * over the ghosted box; cells are independent, so the z planes are split
+ * over the setup threads (orc_set_threads). */
+int orc_fill_michel(const orc_params *p, const orc_michel_config *c,
+                    const orc_box *b, double *state)
+{
+    MichelFill *f = (MichelFill *)calloc(1, sizeof(MichelFill));
+    f->p = p;
+    f->c = c;
+    f->b = b;
+    f->state = state;
+    const int n = parallel_z(b->glo[2], b->ghi[2], michel_fill_job, f, 256);
+    int status = ORC_OK;
+    for (int q = 0; q < n && status == ORC_OK; ++q)
+        status = f->status[q];
+    free(f);
+    return status;
 }
 
 /* compute_diagnostics, Examples/GRHDLevelDataKerrSchildDisk/

@@ -18,6 +18,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _ORACLE_DIR = os.path.join(os.path.dirname(_HERE), "oracle")
 _LIB_PATH = os.path.join(_ORACLE_DIR, "liborc_grhd.so")
+# the same source built for timing (-O3, FMA contraction allowed)
+_FAST_LIB_PATH = os.path.join(_ORACLE_DIR, "liborc_grhd_fast.so")
 
 NCOMP = 11
 D, S1, S2, S3, TAU, RHO, EPS, PRESS, V1, V2, V3 = range(11)
@@ -147,82 +149,102 @@ def build():
 
 
 def lib():
+    """The parity build (no FMA contraction): the checker."""
     global _lib
     if _lib is None:
         if not os.path.exists(_LIB_PATH):
             build()
-        L = C.CDLL(_LIB_PATH)
-        P, B = C.POINTER(Params), C.POINTER(Box)
-        dp, i64 = C.POINTER(C.c_double), C.c_int64
-        L.orc_default_params.argtypes = [P]
-        L.orc_background_vars.argtypes = [P, C.c_double, C.c_double,
-                                          C.c_double, C.c_double, dp]
-        L.orc_compute_conserved.argtypes = [P, dp, dp, dp]
-        L.orc_recover_primitive.argtypes = [P, dp, dp, dp,
-                                            C.POINTER(C.c_int), dp]
-        L.orc_muscl_hlle_flux.argtypes = [P, dp, dp, dp, dp, dp, dp,
-                                          C.c_double, dp, C.c_int, dp]
-        L.orc_compute_rhs.argtypes = [P, B, dp, dp, i64, dp, C.c_double,
-                                      C.POINTER(Error)]
-        L.orc_compute_rhs_mdot.argtypes = [P, B, dp, dp, i64, dp,
-                                           C.c_double, dp, C.POINTER(Error)]
-        L.orc_advance_ssprk2_mdot.argtypes = [P, B, dp, dp, C.c_double,
-                                              C.c_double, C.POINTER(Diag),
-                                              C.POINTER(Error), dp]
-        L.orc_advance_rk4_mdot.argtypes = [P, B, dp, dp, C.c_double,
-                                           C.c_double, C.POINTER(Diag),
-                                           C.POINTER(Error), dp]
-        L.orc_compute_rhs_slabs.argtypes = [P, B, dp, dp, i64, dp,
-                                            C.c_double, C.c_int,
-                                            C.POINTER(Error)]
-        L.orc_recover_primitives.argtypes = [P, B, dp, C.c_double,
-                                             C.POINTER(Diag)]
-        L.orc_compute_max_inverse_dt.argtypes = [P, B, dp, dp, C.c_double,
-                                                 dp, C.POINTER(Error)]
-        L.orc_compute_stable_dt.argtypes = [P, B, dp, dp, C.c_double,
-                                            C.c_double, dp, C.POINTER(Error)]
-        L.orc_update_conserved.argtypes = [P, B, dp, dp, i64, C.c_double,
-                                           C.c_double, C.c_int,
-                                           C.POINTER(Diag)]
-        L.orc_advance_ssprk2.argtypes = [P, B, dp, dp, C.c_double,
-                                         C.c_double, C.POINTER(Diag),
-                                         C.POINTER(Error)]
-        L.orc_advance_rk4.argtypes = [P, B, dp, dp, C.c_double, C.c_double,
-                                      C.POINTER(Diag), C.POINTER(Error)]
-        L.orc_default_torus_config.argtypes = [C.POINTER(TorusConfig)]
-        L.orc_make_torus_parameters.argtypes = [P, C.POINTER(TorusConfig), B,
-                                                C.c_double,
-                                                C.POINTER(TorusParams)]
-        L.orc_fill_torus.argtypes = [P, C.POINTER(TorusConfig),
-                                     C.POINTER(TorusParams), B, dp,
-                                     C.c_double]
-        L.orc_michel_constants.argtypes = [C.POINTER(MichelConfig), dp]
-        L.orc_michel_point.argtypes = [P, C.POINTER(MichelConfig), C.c_double,
-                                       dp]
-        L.orc_fill_michel.argtypes = [P, C.POINTER(MichelConfig), B, dp]
-        L.orc_set_threads.argtypes = [C.c_int]
-        L.orc_fill_conserved_from_primitives.argtypes = [P, B, dp,
-                                                         C.c_double]
-        L.orc_disk_diagnostics.argtypes = [P, B, C.c_int * 3, C.c_int * 3, dp,
-                                           C.c_double, dp]
-        K = C.POINTER(KitpConfig)
-        L.orc_kitp_viscous_rhs.argtypes = [P, K, B, dp, dp, i64, C.c_double]
-        L.orc_kitp_sink_rhs.argtypes = [P, K, B, dp, dp, i64, C.c_double]
-        L.orc_kitp_sink_decay.argtypes = [P, K, B, dp, C.c_double,
-                                          C.c_double]
-        L.orc_fill_kitp_disk.argtypes = [P, C.POINTER(KitpDisk), B, dp,
-                                         C.c_double]
-        L.orc_fill_kitp_disk.restype = None
-        L.orc_ccz4_compute_rhs.argtypes = [P, B, dp, dp, i64, dp,
-                                           C.POINTER(Error)]
-        L.orc_ccz4_recover_primitives.argtypes = [P, B, dp, C.POINTER(Diag)]
-        L.orc_ccz4_recover_primitives.restype = None
-        L.orc_ccz4_compute_max_inverse_dt.argtypes = [P, B, dp, dp, dp,
-                                                      C.POINTER(Error)]
-        L.orc_ccz4_fill_from_background.argtypes = [P, B, dp, C.c_double]
-        L.orc_ccz4_fill_from_background.restype = None
-        _lib = L
+        _lib = _bind(C.CDLL(_LIB_PATH))
     return _lib
+
+
+_fast_lib = None
+
+
+def fast_lib():
+    """The timing build of the same source (-O3, AVX2 + FMA): the CPU
+    baseline, and the second correct evaluation of the reference's
+    algorithm in tests/test_oracle_conditioning.py."""
+    global _fast_lib
+    if _fast_lib is None:
+        if not os.path.exists(_FAST_LIB_PATH):
+            build()
+        _fast_lib = _bind(C.CDLL(_FAST_LIB_PATH))
+    return _fast_lib
+
+
+def _bind(L):
+    """Declares the argument types of the oracle's entry points on L."""
+    P, B = C.POINTER(Params), C.POINTER(Box)
+    dp, i64 = C.POINTER(C.c_double), C.c_int64
+    L.orc_default_params.argtypes = [P]
+    L.orc_background_vars.argtypes = [P, C.c_double, C.c_double,
+                                      C.c_double, C.c_double, dp]
+    L.orc_compute_conserved.argtypes = [P, dp, dp, dp]
+    L.orc_recover_primitive.argtypes = [P, dp, dp, dp,
+                                        C.POINTER(C.c_int), dp]
+    L.orc_muscl_hlle_flux.argtypes = [P, dp, dp, dp, dp, dp, dp,
+                                      C.c_double, dp, C.c_int, dp]
+    L.orc_compute_rhs.argtypes = [P, B, dp, dp, i64, dp, C.c_double,
+                                  C.POINTER(Error)]
+    L.orc_compute_rhs_mdot.argtypes = [P, B, dp, dp, i64, dp,
+                                       C.c_double, dp, C.POINTER(Error)]
+    L.orc_advance_ssprk2_mdot.argtypes = [P, B, dp, dp, C.c_double,
+                                          C.c_double, C.POINTER(Diag),
+                                          C.POINTER(Error), dp]
+    L.orc_advance_rk4_mdot.argtypes = [P, B, dp, dp, C.c_double,
+                                       C.c_double, C.POINTER(Diag),
+                                       C.POINTER(Error), dp]
+    L.orc_compute_rhs_slabs.argtypes = [P, B, dp, dp, i64, dp,
+                                        C.c_double, C.c_int,
+                                        C.POINTER(Error)]
+    L.orc_recover_primitives.argtypes = [P, B, dp, C.c_double,
+                                         C.POINTER(Diag)]
+    L.orc_compute_max_inverse_dt.argtypes = [P, B, dp, dp, C.c_double,
+                                             dp, C.POINTER(Error)]
+    L.orc_compute_stable_dt.argtypes = [P, B, dp, dp, C.c_double,
+                                        C.c_double, dp, C.POINTER(Error)]
+    L.orc_update_conserved.argtypes = [P, B, dp, dp, i64, C.c_double,
+                                       C.c_double, C.c_int,
+                                       C.POINTER(Diag)]
+    L.orc_advance_ssprk2.argtypes = [P, B, dp, dp, C.c_double,
+                                     C.c_double, C.POINTER(Diag),
+                                     C.POINTER(Error)]
+    L.orc_advance_rk4.argtypes = [P, B, dp, dp, C.c_double, C.c_double,
+                                  C.POINTER(Diag), C.POINTER(Error)]
+    L.orc_default_torus_config.argtypes = [C.POINTER(TorusConfig)]
+    L.orc_make_torus_parameters.argtypes = [P, C.POINTER(TorusConfig), B,
+                                            C.c_double,
+                                            C.POINTER(TorusParams)]
+    L.orc_fill_torus.argtypes = [P, C.POINTER(TorusConfig),
+                                 C.POINTER(TorusParams), B, dp,
+                                 C.c_double]
+    L.orc_michel_constants.argtypes = [C.POINTER(MichelConfig), dp]
+    L.orc_michel_point.argtypes = [P, C.POINTER(MichelConfig), C.c_double,
+                                   dp]
+    L.orc_fill_michel.argtypes = [P, C.POINTER(MichelConfig), B, dp]
+    L.orc_set_threads.argtypes = [C.c_int]
+    L.orc_fill_conserved_from_primitives.argtypes = [P, B, dp,
+                                                     C.c_double]
+    L.orc_disk_diagnostics.argtypes = [P, B, C.c_int * 3, C.c_int * 3, dp,
+                                       C.c_double, dp]
+    K = C.POINTER(KitpConfig)
+    L.orc_kitp_viscous_rhs.argtypes = [P, K, B, dp, dp, i64, C.c_double]
+    L.orc_kitp_sink_rhs.argtypes = [P, K, B, dp, dp, i64, C.c_double]
+    L.orc_kitp_sink_decay.argtypes = [P, K, B, dp, C.c_double,
+                                      C.c_double]
+    L.orc_fill_kitp_disk.argtypes = [P, C.POINTER(KitpDisk), B, dp,
+                                     C.c_double]
+    L.orc_fill_kitp_disk.restype = None
+    L.orc_ccz4_compute_rhs.argtypes = [P, B, dp, dp, i64, dp,
+                                       C.POINTER(Error)]
+    L.orc_ccz4_recover_primitives.argtypes = [P, B, dp, C.POINTER(Diag)]
+    L.orc_ccz4_recover_primitives.restype = None
+    L.orc_ccz4_compute_max_inverse_dt.argtypes = [P, B, dp, dp, dp,
+                                                  C.POINTER(Error)]
+    L.orc_ccz4_fill_from_background.argtypes = [P, B, dp, C.c_double]
+    L.orc_ccz4_fill_from_background.restype = None
+    return L
 
 
 def _dp(a: np.ndarray):

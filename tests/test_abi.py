@@ -104,3 +104,18 @@ def test_header_is_plain_c_and_ctypes_layouts_match(tmp_path):
             assert C.sizeof(cls) == int(value), cname
         else:
             assert getattr(cls, what).offset == int(value), (cname, what)
+
+
+def test_cxx_dropin_compiles_and_links(tmp_path):
+    """tests/cxx_dropin.cpp -- the C++ drop-in operator class a maintainer
+    writes over the header -- compiles warning-free with g++ and links
+    against the built library (run on a GPU by
+    tests/test_gpu_cxx_dropin.py)."""
+    import shutil
+    import cases
+    if shutil.which("g++") is None:
+        pytest.skip("no C++ compiler")
+    from grdzhadzha_b200 import _lib as L
+    if not os.path.exists(L.LIB_PATH):
+        pytest.fail(f"{L.LIB_PATH} not built")
+    assert os.path.exists(cases.build_cxx_dropin(tmp_path))

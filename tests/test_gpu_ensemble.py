@@ -168,3 +168,38 @@ def test_barrier_wait_runs_out_and_ensemble_recovers():
     ref = _single(_members()[:2], 1)
     for i, (_, lv) in enumerate(mem):
         _check_fp64(lv.state.cpu().numpy(), ref[i][0], MEMBERS[i])
+
+
+def test_fp64_ensemble_members_match_oracle():
+    """Members of the persistent launch against the oracle directly: a
+    Michel inflow and an a = 0.9 torus, three RK4 steps in k_ensemble
+    (graph replay) with each member's dt capped at half its CFL step (the
+    cap binds, so the oracle takes the same steps), against the oracle's
+    advance_rk4: conserved state <= 1e-13 of its scale, the three steps'
+    change <= 1e-11 of its scale (the single-box parity tests' bounds),
+    member time exact to rounding."""
+    import grdzhadzha_b200 as G
+    steps = 3
+    names = ["michel_c1", "torus_a09"]
+    cs = [cases.CASES[n]() for n in names]
+    caps = [0.5 * O.stable_dt(p, box, s.copy(), CFL, t)
+            for p, box, s, t in cs]
+    mem = [(cases.gpu_operator(p), cases.gpu_level(box, s))
+           for p, box, s, t in cs]
+    ens = G.Ensemble(mem, cfl=CFL, max_dt=caps)
+    ens.advance(steps, use_graph=True)
+    for i, (p, box, s, t) in enumerate(cs):
+        ref = s.copy()
+        for k in range(steps):
+            O.advance_rk4(p, box, ref, t + k * caps[i], caps[i])
+        got = mem[i][1].state.cpu().numpy().reshape(-1)
+        start = O.interior(box, s)
+        es = cases.rel_err(O.interior(box, got), O.interior(box, ref))
+        ei = cases.rel_err(O.interior(box, got) - start,
+                           O.interior(box, ref) - start)
+        print(f"ensemble member {names[i]} vs oracle: state {es}, "
+              f"change {ei}")
+        assert np.all(es <= 1e-13), (names[i], es)
+        assert np.all(ei <= 1e-11), (names[i], ei)
+        info = ens.member_info(i)
+        assert abs(info["time"] - (t + steps * caps[i])) <= 1e-12 * steps * caps[i]
