@@ -186,6 +186,12 @@ SIGNATURES = {
                                              _dp, C.c_double, C.c_double,
                                              C.c_double, C.c_int, _dp, _dp,
                                              _P(Diagnostics), _vp]),
+    "grhd_advance_rk4_cfl_host": (C.c_int, [_vp, _vp, C.c_int64, _P(Box),
+                                            _dp, C.c_double, C.c_double,
+                                            C.c_double, _dp, _dp,
+                                            _P(Diagnostics),
+                                            _P(C.c_longlong),
+                                            _P(C.c_longlong), _vp]),
     "grhd_ssprk2_stage": (C.c_int, [_vp, C.c_int, _vp, C.c_int64, _vp,
                                     C.c_int64, _P(Box), _dp, C.c_double,
                                     C.c_double, _P(Diagnostics), _vp]),

@@ -41,6 +41,8 @@ struct grhd_ctx
     size_t ccz4_geo_cap = 0;
     double *ccz4_stage = nullptr; // CCZ4 operator: SSPRK2 stage (36 comps)
     size_t ccz4_stage_cap = 0;
+    double *host_state = nullptr; // device copy of a host-held state
+    size_t host_state_cap = 0;
     double *mdot_part = nullptr; // per face-kernel block accretion sums
     size_t mdot_cap = 0;
     double *mdot_acc = nullptr;  // [Mdot of the last RHS, time integral]
@@ -563,6 +565,7 @@ void grhd_destroy(grhd_ctx *ctx)
     cudaFree(ctx->diag_part);
     cudaFree(ctx->ccz4_geo);
     cudaFree(ctx->ccz4_stage);
+    cudaFree(ctx->host_state);
     if (ctx->status_h)
         cudaFreeHost(ctx->status_h);
     for (auto &r : ctx->prof_pending)
@@ -1258,6 +1261,93 @@ int grhd_advance_rk4_cfl(grhd_ctx *ctx, double *state, int64_t state_cs,
     *max_inverse_dt = bits_to_double(ctx->status_h->maxinv_bits);
     if (dt_used)
         *dt_used = dt;
+    return GRHD_OK;
+}
+
+// One grhd_advance_rk4_cfl step of a state held in host memory.  Host ->
+// device goes what the step reads: the conserved components of every cell
+// (the box is the whole domain, so every ghost is physical and refilled
+// from the interior), the primitives of the z planes that hold excised
+// cells (frozen stencil neighbours), and in mixed precision the pressure
+// (con2prim's starting point).  Device -> host goes the whole state.
+int grhd_advance_rk4_cfl_host(grhd_ctx *ctx, double *host_state,
+                              int64_t state_cs, const grhd_box *box,
+                              const double inverse_dx[3], double time,
+                              double cfl, double max_dt,
+                              double *max_inverse_dt, double *dt_used,
+                              grhd_diagnostics *diag, long long *h2d_bytes,
+                              long long *d2h_bytes, void *stream)
+{
+    if (!ctx)
+        return GRHD_ERR_INVALID_ARG;
+    std::memset(&ctx->last_error, 0, sizeof(ctx->last_error));
+    if (!host_state || !box || !valid_box(box) || !box_is_domain(box))
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "host step needs a host state and a box covering "
+                         "the whole domain");
+    GRHD_CUDA(ctx, cudaSetDevice(ctx->device));
+    const BoxDev b = make_box(box, state_cs);
+    int st = check_strides(ctx, b, state_cs, -1);
+    if (st)
+        return st;
+    if ((st = grow(ctx, &ctx->host_state, &ctx->host_state_cap,
+                   kStateComps * (size_t)state_cs)))
+        return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    double *dev = ctx->host_state;
+    const size_t cs = (size_t)state_cs;
+    long long in = 0;
+    GRHD_CUDA(ctx, cudaMemcpyAsync(dev, host_state, 5 * cs * sizeof(double),
+                                   cudaMemcpyHostToDevice, s));
+    in += 5 * cs * sizeof(double);
+    const bool mixed = ctx->params.precision == GRHD_PRECISION_MIXED;
+    if (mixed)
+    {
+        GRHD_CUDA(ctx, cudaMemcpyAsync(dev + kPress * cs,
+                                       host_state + kPress * cs,
+                                       cs * sizeof(double),
+                                       cudaMemcpyHostToDevice, s));
+        in += cs * sizeof(double);
+    }
+    const double R = ctx->params.excision_radius;
+    if (R > 0.0)
+    {
+        // ghosted z planes with a cell centre inside |z| < R, one plane of
+        // margin each side
+        const double dx = ctx->params.dx, cz = ctx->params.center[2];
+        int k0 = (int)std::floor((cz - R) / dx - 0.5) - 1;
+        int k1 = (int)std::ceil((cz + R) / dx - 0.5) + 1;
+        k0 = std::max(k0, b.glo[2]);
+        k1 = std::min(k1, b.ghi[2]);
+        if (k0 <= k1)
+        {
+            const size_t plane = (size_t)b.gn[0] * b.gn[1];
+            const size_t off = (size_t)(k0 - b.glo[2]) * plane;
+            const size_t n = (size_t)(k1 - k0 + 1) * plane;
+            for (int c = 5; c < kStateComps; ++c)
+            {
+                if (mixed && c == kPress)
+                    continue;
+                GRHD_CUDA(ctx, cudaMemcpyAsync(dev + c * cs + off,
+                                               host_state + c * cs + off,
+                                               n * sizeof(double),
+                                               cudaMemcpyHostToDevice, s));
+                in += n * sizeof(double);
+            }
+        }
+    }
+    st = grhd_advance_rk4_cfl(ctx, dev, state_cs, box, inverse_dx, time, cfl,
+                              max_dt, max_inverse_dt, dt_used, diag, stream);
+    if (st)
+        return st;
+    GRHD_CUDA(ctx, cudaMemcpyAsync(host_state, dev,
+                                   kStateComps * cs * sizeof(double),
+                                   cudaMemcpyDeviceToHost, s));
+    GRHD_CUDA(ctx, cudaStreamSynchronize(s));
+    if (h2d_bytes)
+        *h2d_bytes = in;
+    if (d2h_bytes)
+        *d2h_bytes = (long long)(kStateComps * cs * sizeof(double));
     return GRHD_OK;
 }
 

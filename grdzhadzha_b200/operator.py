@@ -586,6 +586,32 @@ class _OperatorBase:
             C.byref(mi), C.byref(tout), C.byref(d), _stream()))
         return tout.value, mi.value, d
 
+    def advance_rk4_cfl_host(self, host_state, box, cfl, time=0.0,
+                             max_dt=0.0, max_inverse_dt=0.0,
+                             inverse_dx_U=None):
+        """New: advance_rk4_cfl of a state in host memory
+        (grhd_advance_rk4_cfl_host): host_state is a CPU float64 tensor of
+        the whole-domain LevelBox `box`'s shape (pinned for fast copies),
+        updated in place.  Returns (dt, next max_inverse_dt, diagnostics,
+        host-to-device bytes, device-to-host bytes)."""
+        if not cfl > 0.0:
+            raise L.InvalidArgument(L.GRHD_ERR_INVALID_ARG, None)
+        if host_state.device.type != "cpu" or \
+                host_state.dtype != torch.float64 or \
+                not host_state.is_contiguous():
+            raise L.InvalidArgument(L.GRHD_ERR_INVALID_ARG, None)
+        mi = C.c_double(max_inverse_dt)
+        dt = C.c_double()
+        d = L.Diagnostics()
+        hb, db = C.c_longlong(), C.c_longlong()
+        b = box.c_box()
+        self._check(self._lib.grhd_advance_rk4_cfl_host(
+            self._ctx, C.c_void_p(host_state.data_ptr()),
+            host_state[0].numel(), C.byref(b), self._inv(inverse_dx_U),
+            time, cfl, max_dt, C.byref(mi), C.byref(dt), C.byref(d),
+            C.byref(hb), C.byref(db), _stream()))
+        return dt.value, mi.value, d, hb.value, db.value
+
 
 class FixedBGLevelDataFiniteVolumeOperator(_OperatorBase):
     """FixedBGFArrayBoxFiniteVolume.hpp:446-614 (static background)."""

@@ -284,6 +284,25 @@ int grhd_advance_rk4_cfl_steps(grhd_ctx *ctx, double *state,
                                double *max_inverse_dt, double *time_out,
                                grhd_diagnostics *diag, void *stream);
 
+/* New: grhd_advance_rk4_cfl of a state held in HOST memory (host_state:
+ * the whole-domain box's 11 components at host_state + c * stride; pinned
+ * memory copies fastest).  The call copies to the device what the step
+ * reads -- the 5 conserved components of every cell, the primitive
+ * components of the z planes that hold excised cells, and in mixed
+ * precision the pressure -- runs the step there (the same kernels as
+ * grhd_advance_rk4_cfl, same results bit for bit) and copies all 11
+ * components back; the other primitive components on input are ignored.
+ * h2d_bytes / d2h_bytes (may be NULL) receive the bytes moved each way.
+ * The device copy of the state lives in the context.  Synchronous. */
+int grhd_advance_rk4_cfl_host(grhd_ctx *ctx, double *host_state,
+                              int64_t state_comp_stride,
+                              const grhd_box *box,
+                              const double inverse_dx[3], double time,
+                              double cfl, double max_dt,
+                              double *max_inverse_dt, double *dt_used,
+                              grhd_diagnostics *diag, long long *h2d_bytes,
+                              long long *d2h_bytes, void *stream);
+
 /* ---- pointwise kernels for verification ---- */
 
 /* ADM background vars at n points (xyz[3n], positions relative to the

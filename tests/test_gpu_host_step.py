@@ -1,0 +1,76 @@
+"""grhd_advance_rk4_cfl_host (new): one CFL-limited RK4 step of a state in
+host memory, against grhd_advance_rk4_cfl on the same state in device
+memory.  The host call copies to the device only what the step reads (the
+conserved components, the primitives of the z planes holding excised
+cells, the pressure in mixed precision), so the test poisons every other
+primitive slot of the host state with NaN: the results must still equal
+the device call's bit for bit (both run the same kernels on the same
+inputs), in FP64 and in mixed precision, over two steps."""
+import numpy as np
+import pytest
+
+import cases
+import oracle_lib as O
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+
+def _excised_planes(p, box):
+    """Ghosted z-plane indices of the state array that hold excised cells
+    or their one-plane margin (as the entry point copies them)."""
+    R, dx, cz = p.excision_radius, p.dx, p.center[2]
+    k0 = int(np.floor((cz - R) / dx - 0.5)) - 1
+    k1 = int(np.ceil((cz + R) / dx - 0.5)) + 1
+    k0, k1 = max(k0, box.glo[2]), min(k1, box.ghi[2])
+    return slice(k0 - box.glo[2], k1 - box.glo[2] + 1)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", ["torus_a09", "michel_c1"])
+def test_host_step_equals_device_step(name, precision):
+    p, box, s, t = cases.CASES[name]()
+    assert p.excision_radius > 0.0
+    op = cases.gpu_operator(p, precision=precision)
+    lv = cases.gpu_level(box, s)
+    host = torch.from_numpy(s.copy()).reshape(lv.state.shape).pin_memory()
+    V = host.numpy()
+    keep = _excised_planes(p, box)
+    for c in range(5, 11):
+        if precision == "mixed" and c == O.PRESS:
+            continue
+        poisoned = np.full_like(V[c], np.nan)
+        poisoned[keep] = V[c][keep]
+        V[c] = poisoned
+    mi_d = mi_h = 0.0
+    for _ in range(2):
+        dt_d, mi_d, d_d = op.advance_rk4_cfl(lv, 0.25, time=t,
+                                             max_inverse_dt=mi_d)
+        dt_h, mi_h, d_h, hb, db = op.advance_rk4_cfl_host(
+            host, lv, 0.25, time=t, max_inverse_dt=mi_h)
+        assert dt_h == dt_d and mi_h == mi_d
+        assert (d_h.num_cells, d_h.num_conserved_resets) == \
+            (d_d.num_cells, d_d.num_conserved_resets)
+        t += dt_d
+    dev = lv.state.cpu()
+    assert torch.isfinite(host).all()
+    assert torch.equal(host, dev), (host - dev).abs().max()
+    n = lv.state[0].numel()
+    plane = lv.state.shape[2] * lv.state.shape[3]
+    nplanes = keep.stop - keep.start
+    want_in = 8 * (5 * n + (n if precision == "mixed" else 0)
+                   + (6 - (precision == "mixed")) * nplanes * plane)
+    assert hb == want_in and db == 8 * 11 * n, (hb, db, want_in)
+
+
+def test_host_step_rejects_a_box_that_is_not_the_domain():
+    import grdzhadzha_b200 as G
+    p, _, _, _ = cases.CASES["fixedbg"]()
+    op = cases.gpu_operator(p)
+    lv = G.LevelBox(lo=(0, 0, 0), hi=(7, 7, 7), ghost=2,
+                    domain_lo=(0, 0, 0), domain_hi=(15, 15, 15),
+                    device="cuda")
+    host = lv.state.cpu()
+    with pytest.raises(G.InvalidArgument):
+        op.advance_rk4_cfl_host(host, lv, 0.25)
