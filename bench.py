@@ -393,8 +393,45 @@ def run_adjoint(n, steps, every, fd_steps, hbm_peak):
         "backward_over_forward": bwd / fwd,
         "forward_cell_updates_per_s": cells * steps / (fwd / 1e3),
         "gpu_launches": adj.launch_count() - l0})
+    # the adjoint checked without differences: the tangent-linear sweep
+    # along the same steps and branches gives dJ.v, which must equal
+    # <gradient, v>; over the whole run for a random direction (relative
+    # to sum_k |g_k v_k|), and per parameter over the first 25 steps
+    import numpy as np
+    rng = np.random.default_rng(20261203)
+    checks = []
+    v = list(rng.uniform(-1.0, 1.0, 8))
+    ev[0].record()
+    _, dJ = adj.tangent(v)
+    ev[1].record()
+    torch.cuda.synchronize()
+    out["tangent_sweep_ms"] = ev[0].elapsed_time(ev[1])
+    want = float(np.dot(grad, v))
+    scale = float(np.abs(np.asarray(grad) * np.asarray(v)).sum())
+    checks.append({"steps": steps, "direction": "random",
+                   "tangent": dJ, "adjoint": want,
+                   "rel_err": abs(dJ - want) / scale})
     del adj, op
     torch.cuda.empty_cache()
+    short = min(25, steps)
+    for R in (2.5, 5.0):
+        op, adj = W.adjoint_torus(n=n, steps=short, checkpoint_every=short,
+                                  accretion_radius=R)
+        adj.forward()
+        g = adj.backward()
+        for k, name in enumerate(THETA_NAMES):
+            e = [0.0] * 8
+            e[k] = 1.0
+            _, dJ = adj.tangent(e)
+            checks.append({"steps": short, "accretion_radius": R,
+                           "direction": name, "tangent": dJ,
+                           "adjoint": g[k],
+                           "rel_err": abs(dJ - g[k]) / max(abs(g[k]), 1e-300),
+                           "rel_err_of_norm": abs(dJ - g[k]) / max(
+                               float(np.linalg.norm(g)), 1e-300)})
+        del adj, op
+        torch.cuda.empty_cache()
+    out["tlm_check"] = checks
     if fd_steps > 0:
         op, adj = W.adjoint_torus(n=n, steps=fd_steps,
                                   checkpoint_every=min(every, fd_steps),
@@ -848,8 +885,14 @@ def main():
                     line["adjoint_fd_max_rel_err"] = max(
                         r["rel_err"][0] for r in rows.values())
                 if "tlm_check" in adj:
-                    line["adjoint_tlm_max_rel_err"] = max(
-                        c["rel_err"] for c in adj["tlm_check"])
+                    line["adjoint_tlm_rel_err_400_steps"] = next(
+                        c["rel_err"] for c in adj["tlm_check"]
+                        if c["direction"] == "random")
+                    for R in (2.5, 5.0):
+                        line[f"adjoint_tlm_max_rel_err_of_norm_25_steps_r{R}"] \
+                            = max(c["rel_err_of_norm"]
+                                  for c in adj["tlm_check"]
+                                  if c.get("accretion_radius") == R)
             line["variants"] = variants
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -299,6 +299,8 @@ SIGNATURES = {
                                             C.c_int64, _vp, C.c_int64, _vp]),
     "grhd_adjoint_forward": (C.c_int, [_vp, _P(AdjointTorus), _dp, _vp]),
     "grhd_adjoint_backward": (C.c_int, [_vp, _dp, _vp, C.c_int64, _vp]),
+    "grhd_adjoint_tangent": (C.c_int, [_vp, _P(AdjointTorus), _dp, _dp, _dp,
+                                       _vp]),
     "grhd_adjoint_rhs_vjp": (C.c_int, [_vp, _vp, C.c_int64, _vp, C.c_int64,
                                        C.c_double, _vp, C.c_int64, _dp,
                                        _vp]),

@@ -109,6 +109,18 @@ class TorusAccretionAdjoint:
                                                     _stream()))
         return list(g)
 
+    def tangent(self, direction, theta=None) -> tuple:
+        """Tangent-linear sweep (grhd_adjoint_tangent): (J, dJ) with dJ =
+        sum_k direction[k] dJ/dtheta_k along the same discrete steps and
+        branches as the adjoint, so dJ = <backward(), direction> to
+        rounding.  Overwrites the forward's tape."""
+        t = self.torus_of(self.theta() if theta is None else theta)
+        v = (C.c_double * 8)(*[float(x) for x in direction])
+        J, dJ = C.c_double(), C.c_double()
+        self._check(self._lib.grhd_adjoint_tangent(
+            self._h, C.byref(t), v, C.byref(J), C.byref(dJ), _stream()))
+        return J.value, dJ.value
+
     def initial_state(self, theta=None, level: LevelBox | None = None):
         lv = level or LevelBox(lo=self.level.lo, hi=self.level.hi,
                                ghost=self.level.ghost,

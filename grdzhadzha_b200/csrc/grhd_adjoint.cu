@@ -35,6 +35,7 @@
 #include "grhd_adjoint.cuh"
 #include "grhd_adjoint_items.cuh"
 #include "grhd_b200.h"
+#include "grhd_tangent.cuh"
 #include "grhd_host.cuh"
 #include "grhd_kernels.cuh"
 
@@ -42,6 +43,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <utility>
 #include <vector>
 
 using namespace grhd;
@@ -164,6 +166,68 @@ __global__ void __launch_bounds__(kAdjThreads)
         torus_tangent_item(T, lam, tangent, tcs, t, acc);
     for (int p = 0; p < 8; ++p)
         block_add(acc[p], slots + (int64_t)p * gridDim.x);
+}
+
+// ------------------------------------------------ tangent-linear kernels
+
+__global__ void __launch_bounds__(kAdjThreads) k_tan_cells(TanRhs A)
+{
+    const int64_t n = A.b.ivol();
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x)
+        tan_cell_item(A, t);
+}
+
+__global__ void __launch_bounds__(256) k_tan_ghosts(TanRhs A)
+{
+    const int64_t n = A.b.gvol();
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n;
+         g += (int64_t)gridDim.x * blockDim.x)
+        tan_ghost_item(A, g);
+}
+
+__global__ void __launch_bounds__(kAdjThreads) k_tan_rhs(TanRhs A,
+                                                         double *slot)
+{
+    const int64_t n = A.b.ivol();
+    double m = 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x)
+        m += tan_rhs_item(A, t);
+    block_add(m, slot);
+}
+
+__global__ void __launch_bounds__(256)
+    k_tan_stage(BoxDev b, Options o, double M, double a, double da, int stage,
+                double dt, const double *dUn, const double *dk, double *dacc,
+                const double *Y, const double *pY, const unsigned char *br,
+                double *out)
+{
+    const int64_t n = b.ivol();
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x)
+        tan_stage_item(b, o, M, a, da, stage, dt, dUn, dk, dacc, Y, pY, br,
+                       out, t);
+}
+
+struct Direction
+{
+    double v[8];
+};
+
+// dU0 = sum_k v_k dU0/dtheta_k over the interior (tan0: [8][5][n]).
+__global__ void __launch_bounds__(256)
+    k_tan_combine(int64_t n, const double *tan0, Direction v, double *dU)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x)
+        for (int q = 0; q < 5; ++q)
+        {
+            double s = 0.0;
+            for (int k = 0; k < 8; ++k)
+                s += v.v[k] * tan0[((int64_t)k * 5 + q) * n + t];
+            dU[q * n + t] = s;
+        }
 }
 
 size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
@@ -797,6 +861,112 @@ int grhd_adjoint_backward(grhd_adjoint *a, double grad[8], double *lambda0,
             return rc;
         ADJ_CUDA(a, cudaStreamSynchronize(s));
     }
+    return GRHD_OK;
+}
+
+// Tangent-linear sweep: J and dJ = (dJ/dtheta) . direction along the same
+// taped forward steps as grhd_adjoint_forward (each step's tape rebuilt and
+// differentiated in forward mode, no checkpoints needed).  The buffers of
+// the sweep are allocated and freed per call.
+int grhd_adjoint_tangent(grhd_adjoint *a, const grhd_adjoint_torus *t,
+                         const double direction[8], double *J, double *dJ,
+                         void *stream)
+{
+    if (!a || !t || !direction || !dJ)
+        return GRHD_ERR_INVALID_ARG;
+    if (!a->arena)
+        return adj_error(a, GRHD_ERR_INVALID_ARG, "adjoint not created");
+    cudaStream_t s = (cudaStream_t)stream;
+    ADJ_CUDA(a, cudaSetDevice(a->device));
+    TorusArgs T;
+    int rc = make_torus_args(a, t, T);
+    if (rc)
+        return rc;
+    a->bg.a = t->spin;
+    // the previous forward's tape and checkpoints are overwritten
+    a->have_forward = false;
+    const BoxDev &b = a->b;
+    const int64_t ni = b.ivol(), gv = b.gvol();
+    const size_t n5 = 5 * (size_t)ni;
+    double *buf = nullptr;
+    const size_t total = 8 * n5 + 6 * n5 + 5 * (size_t)gv + a->grid;
+    ADJ_CUDA(a, cudaMalloc((void **)&buf, total * sizeof(double)));
+    double *tan0 = buf;
+    double *dUn = tan0 + 8 * n5, *dUs = dUn + n5, *dUx = dUs + n5;
+    double *dS = dUx + n5, *dk = dS + n5, *dacc = dk + n5;
+    double *dP = dacc + n5;
+    double *slots = dP + 5 * (size_t)gv;
+    auto fail = [&](int code) {
+        cudaFree(buf);
+        return code;
+    };
+    k_adj_torus_fill<<<grid_of(gv, 256, 148 * 16), 256, 0, s>>>(
+        T, a->slots[0].U[0]);
+    k_adj_torus_tangent<<<a->grid, kAdjThreads, 0, s>>>(T, nullptr, tan0, ni,
+                                                        a->tan_slots);
+    Direction v;
+    for (int k = 0; k < 8; ++k)
+        v.v[k] = direction[k];
+    const int gi = grid_of(ni, 256, 148 * 16), gg = grid_of(gv, 256, 148 * 16);
+    k_tan_combine<<<gi, 256, 0, s>>>(ni, tan0, v, dUn);
+    a->launches += 3;
+    if (cudaMemsetAsync(slots, 0, a->grid * sizeof(double), s) != cudaSuccess ||
+        cudaMemsetAsync(a->mdot_acc, 0, 2 * sizeof(double), s) != cudaSuccess)
+        return fail(adj_error(a, GRHD_ERR_CUDA, "tangent set-up failed"));
+    if ((rc = reset_status(a, s)))
+        return fail(rc);
+    grhd_adjoint::Slot &sl = a->slots[0];
+    for (int n = 0; n < a->steps; ++n)
+    {
+        forward_step(a, sl, a->Xend, s);
+        for (int st = 0; st < 4; ++st)
+        {
+            TanRhs R;
+            R.b = b;
+            R.o = a->o;
+            R.M = a->bg.M;
+            R.a = a->bg.a;
+            R.da = direction[2];
+            for (int d = 0; d < 3; ++d)
+                R.inv_dx[d] = a->inv_dx[d];
+            R.U = sl.U[st];
+            R.P = sl.P[st];
+            R.bits = sl.bits[st];
+            R.dU = st == 0 ? dUn : dUs;
+            R.dP = dP;
+            R.dS = dS;
+            R.dk = dk;
+            R.mu = a->dt / 6.0 * stage_weight(st);
+            k_tan_cells<<<a->grid, kAdjThreads, 0, s>>>(R);
+            k_tan_ghosts<<<gg, 256, 0, s>>>(R);
+            k_tan_rhs<<<a->grid, kAdjThreads, 0, s>>>(R, slots);
+            k_tan_stage<<<gi, 256, 0, s>>>(b, a->o, a->bg.M, a->bg.a,
+                                           direction[2], st, a->dt, dUn, dk,
+                                           dacc, sl.Y[st], sl.pY[st],
+                                           sl.br[st], st < 3 ? dUs : dUx);
+            a->launches += 4;
+        }
+        if (cudaMemcpyAsync(sl.U[0], a->Xend,
+                            kStateComps * gv * sizeof(double),
+                            cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            return fail(adj_error(a, GRHD_ERR_CUDA, "tangent step copy"));
+        std::swap(dUn, dUx);
+    }
+    if (cudaGetLastError() != cudaSuccess)
+        return fail(adj_error(a, GRHD_ERR_CUDA, "tangent kernel launch"));
+    double acc[2];
+    if (cudaMemcpyAsync(acc, a->mdot_acc, sizeof(acc), cudaMemcpyDeviceToHost,
+                        s) != cudaSuccess)
+        return fail(adj_error(a, GRHD_ERR_CUDA, "tangent read-back"));
+    if ((rc = check_status(a, s)))
+        return fail(rc);
+    double d = 0.0;
+    if ((rc = sum_slots(a, slots, a->grid, &d, s)))
+        return fail(rc);
+    cudaFree(buf);
+    if (J)
+        *J = acc[1];
+    *dJ = d;
     return GRHD_OK;
 }
 

@@ -766,6 +766,17 @@ int grhd_adjoint_forward(grhd_adjoint *adj, const grhd_adjoint_torus *torus,
  * components over the interior, may be NULL) = dJ/dU0.  Synchronous. */
 int grhd_adjoint_backward(grhd_adjoint *adj, double grad[8], double *lambda0,
                           int64_t lambda_comp_stride, void *stream);
+/* Tangent-linear sweep (forward mode): J and dJ = sum_k direction[k]
+ * dJ/dtheta_k for the torus `torus`, along the same taped forward steps
+ * as grhd_adjoint_forward, with the same recorded limiter branches and the
+ * same branch decisions as the backward sweep, so that dJ equals the
+ * gradient's projection <grad, direction> to rounding for every direction
+ * -- the check of the adjoint that needs no finite-difference step.
+ * Overwrites the last forward's tape (call grhd_adjoint_forward again
+ * before a backward).  Allocates its buffers per call.  Synchronous. */
+int grhd_adjoint_tangent(grhd_adjoint *adj, const grhd_adjoint_torus *torus,
+                         const double direction[8], double *J, double *dJ,
+                         void *stream);
 /* Vector-Jacobian product of one RHS evaluation (grhd_compute_rhs of the
  * FP64 operator with the adjoint's parameters, spin = params.ks_spin):
  * state_bar = (dRHS/dU)^T rhs_bar + mdot_bar dMdot/dU over the interior
