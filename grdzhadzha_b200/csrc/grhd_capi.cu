@@ -43,6 +43,10 @@ struct grhd_ctx
     size_t ccz4_stage_cap = 0;
     double *host_state = nullptr; // device copy of a host-held state
     size_t host_state_cap = 0;
+    double *prim2 = nullptr; // host-buffer step: second primitive cache
+    size_t prim2_cap = 0;
+    cudaStream_t h2d = nullptr, d2h = nullptr; // host-buffer step copies
+    std::vector<cudaEvent_t> pipe_events;
     double *mdot_part = nullptr; // per face-kernel block accretion sums
     size_t mdot_cap = 0;
     double *mdot_acc = nullptr;  // [Mdot of the last RHS, time integral]
@@ -566,6 +570,13 @@ void grhd_destroy(grhd_ctx *ctx)
     cudaFree(ctx->ccz4_geo);
     cudaFree(ctx->ccz4_stage);
     cudaFree(ctx->host_state);
+    cudaFree(ctx->prim2);
+    if (ctx->h2d)
+        cudaStreamDestroy(ctx->h2d);
+    if (ctx->d2h)
+        cudaStreamDestroy(ctx->d2h);
+    for (cudaEvent_t e : ctx->pipe_events)
+        cudaEventDestroy(e);
     if (ctx->status_h)
         cudaFreeHost(ctx->status_h);
     for (auto &r : ctx->prof_pending)
@@ -958,6 +969,191 @@ void enqueue_ccz4_rhs(grhd_ctx *ctx, double *rhs, int64_t rhs_cs,
     ctx->launches += 3;
 }
 
+// ---- the host-buffer RK4 step as a wavefront over z chunks
+
+// Chunk c of n: interior planes k0(c)..k1(c) (len planes from lo[2]); its
+// copies carry the ghosted planes plo(c)..phi(c) (the ghost planes below
+// and above the interior go with the first and the last chunk).
+struct ZChunks
+{
+    int lo2, hi2, glo2, ghi2, len, n;
+    int k0(int c) const { return lo2 + c * len; }
+    int k1(int c) const { return std::min(lo2 + (c + 1) * len - 1, hi2); }
+    int plo(int c) const { return c == 0 ? glo2 : k0(c); }
+    int phi(int c) const { return c == n - 1 ? ghi2 : k1(c); }
+};
+
+ZChunks make_zchunks(const BoxDev &b)
+{
+    ZChunks z;
+    z.lo2 = b.lo[2];
+    z.hi2 = b.hi[2];
+    z.glo2 = b.glo[2];
+    z.ghi2 = b.ghi[2];
+    z.len = std::max(8, (b.in[2] + 7) / 8);
+    z.n = (b.in[2] + z.len - 1) / z.len;
+    return z;
+}
+
+// The interior planes k0..k1 of b as a box of their own (BoxDev::t0).
+BoxDev chunk_view(const BoxDev &b, int k0, int k1)
+{
+    BoxDev v = b;
+    v.lo[2] = k0;
+    v.hi[2] = k1;
+    v.in[2] = k1 - k0 + 1;
+    v.t0 = b.t0 + (int64_t)(k0 - b.lo[2]) * b.in[0] * b.in[1];
+    return v;
+}
+
+int pipe_setup(grhd_ctx *ctx, int nchunks)
+{
+    if (!ctx->h2d)
+        GRHD_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->h2d,
+                                                 cudaStreamNonBlocking));
+    if (!ctx->d2h)
+        GRHD_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->d2h,
+                                                 cudaStreamNonBlocking));
+    while (ctx->pipe_events.size() < 2 * (size_t)nchunks + 1)
+    {
+        cudaEvent_t e;
+        GRHD_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->pipe_events.push_back(e);
+    }
+    return GRHD_OK;
+}
+
+// One RK4 step (the kernels of enqueue_rk4, want_cfl) of the state in
+// pinned host memory `host` through its device copy `dev`, as a wavefront
+// over z chunks.  Iteration w copies chunk w in (on its own stream, all
+// chunks queued at once), computes its con2prim and sources once its copy
+// has landed, then runs RK stage s on chunk w-1-s for s = 0..3: the
+// ghost cells of the chunk's planes, its fluxes, its stage kernel.  Stage
+// s on chunk j reads stage-s primitives two planes into chunks j-1 and
+// j+1; those were written earlier in the same or the previous iteration,
+// and the stages alternate between two primitive caches (stage s reads
+// one and prepares stage s+1's in the other) so that no chunk's stage-s
+// primitives are overwritten before its neighbour's stage-s fluxes have
+// read them.  Chunk j's copy out (every component of its ghosted planes)
+// starts as soon as its last stage is done.  Every cell sees exactly the
+// arithmetic of the whole-box step: the result is bit-identical.  The
+// excised planes ek0..ek1 carry their primitives in (empty when ek0 > ek1).
+template <typename T>
+int enqueue_rk4_host_pipelined(grhd_ctx *ctx, double *host, double *dev,
+                               const BoxDev &b, const double inv_dx[3],
+                               double time, double dt, int ek0, int ek1,
+                               cudaStream_t s, long long &in, long long &out)
+{
+    const ZChunks z = make_zchunks(b);
+    int st = pipe_setup(ctx, z.n);
+    if (st)
+        return st;
+    cudaEvent_t *ev_in = ctx->pipe_events.data();
+    cudaEvent_t *ev_out = ev_in + z.n;
+    cudaEvent_t ev_start = ev_in[2 * z.n];
+    const bool mixed = sizeof(T) != sizeof(double);
+    const size_t cs = (size_t)b.cs;
+    const size_t plane = (size_t)b.gn[0] * b.gn[1];
+    GRHD_CUDA(ctx, cudaEventRecord(ev_start, s));
+    GRHD_CUDA(ctx, cudaStreamWaitEvent(ctx->h2d, ev_start, 0));
+    for (int c = 0; c < z.n; ++c)
+    {
+        const int p0 = z.plo(c), p1 = z.phi(c);
+        for (int q = 0; q < kStateComps; ++q)
+        {
+            int q0 = p0, q1 = p1;
+            if (q >= 5 && !(mixed && q == kPress))
+            {
+                q0 = std::max(ek0, p0);
+                q1 = std::min(ek1, p1);
+                if (q0 > q1)
+                    continue;
+            }
+            const size_t off = (size_t)(q0 - b.glo[2]) * plane;
+            const size_t n = (size_t)(q1 - q0 + 1) * plane;
+            GRHD_CUDA(ctx, cudaMemcpyAsync(dev + q * cs + off,
+                                           host + q * cs + off,
+                                           n * sizeof(double),
+                                           cudaMemcpyHostToDevice, ctx->h2d));
+            in += (long long)(n * sizeof(double));
+        }
+        GRHD_CUDA(ctx, cudaEventRecord(ev_in[c], ctx->h2d));
+    }
+    BoxDev sb = b;
+    sb.cs = b.gvol();
+    const Background bgs[4] = {
+        make_background(ctx->params, time),
+        make_background(ctx->params, time + 0.5 * dt),
+        make_background(ctx->params, time + 0.5 * dt),
+        make_background(ctx->params, time + dt)};
+    T *P[2] = {scratch<T>(ctx->prim), scratch<T>(ctx->prim2)};
+    T *k = scratch<T>(ctx->kbuf), *src = scratch<T>(ctx->src);
+    double *acc = ctx->acc;
+    // a chunk is a few dozen planes: face blocks of 8 planes fill the GPU
+    const int zc = std::min(ctx->zchunk, 8);
+    for (int w = 0; w < z.n + 4; ++w)
+    {
+        if (w < z.n)
+        {
+            GRHD_CUDA(ctx, cudaStreamWaitEvent(s, ev_in[w], 0));
+            const BoxDev v = chunk_view(b, z.k0(w), z.k1(w));
+            Timed t_(ctx, GRHD_K_CELLS, s);
+            launch_cells<T>(dev, P[0], src + v.t0, v, bgs[0], ctx->opt,
+                            ctx->status, s);
+        }
+        for (int sg = 0; sg < 4; ++sg)
+        {
+            const int j = w - 1 - sg;
+            if (j < 0 || j >= z.n)
+                continue;
+            T *pin = P[sg % 2], *pout = P[(sg + 1) % 2];
+            const BoxDev v = chunk_view(b, z.k0(j), z.k1(j));
+            {
+                Timed t_(ctx, GRHD_K_GHOSTS, s);
+                launch_fill_ghost_planes<T>(sg == 0 ? dev : ctx->stage, pin,
+                                            sg == 0 ? b : sb, bgs[sg],
+                                            ctx->opt, ctx->status, z.plo(j),
+                                            z.phi(j), s);
+            }
+            {
+                Timed t_(ctx, GRHD_K_FACES, s);
+                launch_faces<T>(pin, src + v.t0, k + v.t0, v, bgs[sg],
+                                ctx->opt, inv_dx, zc, nullptr, s);
+            }
+            {
+                Timed t_(ctx, GRHD_K_STAGE, s);
+                if (sg < 3)
+                    launch_stage<T>(0, dev, b.cs, nullptr, 0, ctx->stage, sb.cs,
+                                    k + v.t0, acc + v.t0, pout, src + v.t0, 1,
+                                    v, bgs[sg + 1], ctx->opt, sg, dt, false,
+                                    inv_dx, ctx->status, s, pin);
+                else
+                    launch_stage<T>(0, dev, b.cs, nullptr, 0, dev, b.cs,
+                                    k + v.t0, acc + v.t0, pout, nullptr, 0, v,
+                                    bgs[3], ctx->opt, 3, dt, true, inv_dx,
+                                    ctx->status, s, pin);
+            }
+            if (sg == 3)
+            {
+                GRHD_CUDA(ctx, cudaEventRecord(ev_out[j], s));
+                GRHD_CUDA(ctx, cudaStreamWaitEvent(ctx->d2h, ev_out[j], 0));
+                const size_t off = (size_t)(z.plo(j) - b.glo[2]) * plane;
+                const size_t n = (size_t)(z.phi(j) - z.plo(j) + 1) * plane;
+                for (int q = 0; q < kStateComps; ++q)
+                {
+                    GRHD_CUDA(ctx, cudaMemcpyAsync(host + q * cs + off,
+                                                   dev + q * cs + off,
+                                                   n * sizeof(double),
+                                                   cudaMemcpyDeviceToHost,
+                                                   ctx->d2h));
+                    out += (long long)(n * sizeof(double));
+                }
+            }
+        }
+    }
+    return GRHD_OK;
+}
+
 } // namespace
 
 extern "C" {
@@ -1270,6 +1466,10 @@ int grhd_advance_rk4_cfl(grhd_ctx *ctx, double *state, int64_t state_cs,
 // from the interior), the primitives of the z planes that hold excised
 // cells (frozen stencil neighbours), and in mixed precision the pressure
 // (con2prim's starting point).  Device -> host goes the whole state.
+// With the CFL speed given (*max_inverse_dt > 0, as every call after the
+// first passes it) and no accretion-rate integral, the copies overlap the
+// step (enqueue_rk4_host_pipelined); otherwise the state is copied in,
+// stepped and copied out in turn.
 int grhd_advance_rk4_cfl_host(grhd_ctx *ctx, double *host_state,
                               int64_t state_cs, const grhd_box *box,
                               const double inverse_dx[3], double time,
@@ -1285,6 +1485,9 @@ int grhd_advance_rk4_cfl_host(grhd_ctx *ctx, double *host_state,
         return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
                          "host step needs a host state and a box covering "
                          "the whole domain");
+    if (!(cfl > 0.0) || !max_inverse_dt)
+        return set_error(ctx, GRHD_ERR_INVALID_ARG, 0, nullptr, 0.0,
+                         "GRHD CFL number must be positive");
     GRHD_CUDA(ctx, cudaSetDevice(ctx->device));
     const BoxDev b = make_box(box, state_cs);
     int st = check_strides(ctx, b, state_cs, -1);
@@ -1296,11 +1499,60 @@ int grhd_advance_rk4_cfl_host(grhd_ctx *ctx, double *host_state,
     cudaStream_t s = (cudaStream_t)stream;
     double *dev = ctx->host_state;
     const size_t cs = (size_t)state_cs;
-    long long in = 0;
+    const bool mixed = ctx->params.precision == GRHD_PRECISION_MIXED;
+    // ghosted z planes with a cell centre inside |z| < R, one plane of
+    // margin each side (empty: ek0 > ek1)
+    int ek0 = 1, ek1 = 0;
+    const double R = ctx->params.excision_radius;
+    if (R > 0.0)
+    {
+        const double dx = ctx->params.dx, cz = ctx->params.center[2];
+        const int k0 = (int)std::floor((cz - R) / dx - 0.5) - 1;
+        const int k1 = (int)std::ceil((cz + R) / dx - 0.5) + 1;
+        ek0 = std::max(k0, b.glo[2]);
+        ek1 = std::min(k1, b.ghi[2]);
+    }
+    long long in = 0, out = 0;
+    if (*max_inverse_dt > 0.0 && !(ctx->params.accretion_radius > 0.0))
+    {
+        BoxDev bb;
+        if ((st = advance_checks(ctx, dev, state_cs, box, inverse_dx, bb, s)) ||
+            (st = grow(ctx, &ctx->prim2, &ctx->prim2_cap,
+                       5 * (size_t)bb.gvol())))
+            return st;
+        double dt = cfl / std::fmax(*max_inverse_dt, 1.0e-14);
+        if (max_dt > 0.0)
+            dt = std::fmin(dt, max_dt);
+        st = mixed ? enqueue_rk4_host_pipelined<float>(
+                         ctx, host_state, dev, bb, inverse_dx, time, dt, ek0,
+                         ek1, s, in, out)
+                   : enqueue_rk4_host_pipelined<double>(
+                         ctx, host_state, dev, bb, inverse_dx, time, dt, ek0,
+                         ek1, s, in, out);
+        // no copy into the caller's memory may outlive the call
+        const cudaError_t e_out = cudaStreamSynchronize(ctx->d2h);
+        const cudaError_t e_in = cudaStreamSynchronize(ctx->h2d);
+        if (st)
+            return st;
+        GRHD_CUDA(ctx, e_out);
+        GRHD_CUDA(ctx, e_in);
+        st = finish_status(ctx, bb, dev, make_background(ctx->params, time),
+                           s);
+        read_diag(ctx, diag);
+        if (st)
+            return st;
+        *max_inverse_dt = bits_to_double(ctx->status_h->maxinv_bits);
+        if (dt_used)
+            *dt_used = dt;
+        if (h2d_bytes)
+            *h2d_bytes = in;
+        if (d2h_bytes)
+            *d2h_bytes = out;
+        return GRHD_OK;
+    }
     GRHD_CUDA(ctx, cudaMemcpyAsync(dev, host_state, 5 * cs * sizeof(double),
                                    cudaMemcpyHostToDevice, s));
     in += 5 * cs * sizeof(double);
-    const bool mixed = ctx->params.precision == GRHD_PRECISION_MIXED;
     if (mixed)
     {
         GRHD_CUDA(ctx, cudaMemcpyAsync(dev + kPress * cs,
@@ -1309,31 +1561,20 @@ int grhd_advance_rk4_cfl_host(grhd_ctx *ctx, double *host_state,
                                        cudaMemcpyHostToDevice, s));
         in += cs * sizeof(double);
     }
-    const double R = ctx->params.excision_radius;
-    if (R > 0.0)
+    if (ek0 <= ek1)
     {
-        // ghosted z planes with a cell centre inside |z| < R, one plane of
-        // margin each side
-        const double dx = ctx->params.dx, cz = ctx->params.center[2];
-        int k0 = (int)std::floor((cz - R) / dx - 0.5) - 1;
-        int k1 = (int)std::ceil((cz + R) / dx - 0.5) + 1;
-        k0 = std::max(k0, b.glo[2]);
-        k1 = std::min(k1, b.ghi[2]);
-        if (k0 <= k1)
+        const size_t plane = (size_t)b.gn[0] * b.gn[1];
+        const size_t off = (size_t)(ek0 - b.glo[2]) * plane;
+        const size_t n = (size_t)(ek1 - ek0 + 1) * plane;
+        for (int c = 5; c < kStateComps; ++c)
         {
-            const size_t plane = (size_t)b.gn[0] * b.gn[1];
-            const size_t off = (size_t)(k0 - b.glo[2]) * plane;
-            const size_t n = (size_t)(k1 - k0 + 1) * plane;
-            for (int c = 5; c < kStateComps; ++c)
-            {
-                if (mixed && c == kPress)
-                    continue;
-                GRHD_CUDA(ctx, cudaMemcpyAsync(dev + c * cs + off,
-                                               host_state + c * cs + off,
-                                               n * sizeof(double),
-                                               cudaMemcpyHostToDevice, s));
-                in += n * sizeof(double);
-            }
+            if (mixed && c == kPress)
+                continue;
+            GRHD_CUDA(ctx, cudaMemcpyAsync(dev + c * cs + off,
+                                           host_state + c * cs + off,
+                                           n * sizeof(double),
+                                           cudaMemcpyHostToDevice, s));
+            in += n * sizeof(double);
         }
     }
     st = grhd_advance_rk4_cfl(ctx, dev, state_cs, box, inverse_dx, time, cfl,

@@ -242,17 +242,13 @@ __device__ __forceinline__ bool shell_cell(const BoxDev &b, int64_t t, int &i,
 // them keeps its frozen primitives, as it does as an interior cell, so a
 // level's RHS does not depend on how it is cut into boxes.
 template <typename T, bool CG = false>
-__device__ __forceinline__ void ghost_item(double *__restrict__ state,
-                                           T *__restrict__ prim,
-                                           const BoxDev &b,
-                                           const Background &bg,
-                                           const Options &o, DevStatus *st,
-                                           int64_t t)
+__device__ __forceinline__ void ghost_at(double *__restrict__ state,
+                                         T *__restrict__ prim,
+                                         const BoxDev &b, const Background &bg,
+                                         const Options &o, DevStatus *st,
+                                         int i, int j, int k)
 {
     {
-        int i, j, k;
-        if (!shell_cell(b, t, i, j, k))
-            return;
         const int iv[3] = {i, j, k};
         int srcc[3] = {i, j, k};
         bool ghost = false;
@@ -315,6 +311,19 @@ __device__ __forceinline__ void ghost_item(double *__restrict__ state,
     }
 }
 
+template <typename T, bool CG = false>
+__device__ __forceinline__ void ghost_item(double *__restrict__ state,
+                                           T *__restrict__ prim,
+                                           const BoxDev &b,
+                                           const Background &bg,
+                                           const Options &o, DevStatus *st,
+                                           int64_t t)
+{
+    int i, j, k;
+    if (shell_cell(b, t, i, j, k))
+        ghost_at<T, CG>(state, prim, b, bg, o, st, i, j, k);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256)
     k_fill_ghosts(double *__restrict__ state, T *__restrict__ prim, BoxDev b,
@@ -323,6 +332,22 @@ __global__ void __launch_bounds__(256)
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
          t < nshell; t += (int64_t)gridDim.x * blockDim.x)
         ghost_item<T>(state, prim, b, bg, o, st, t);
+}
+
+// The shell cells of the ghosted planes k0..k1 only (plane_shell_cell).
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_fill_ghost_planes(double *__restrict__ state, T *__restrict__ prim,
+                        BoxDev b, Background bg, Options o, DevStatus *st,
+                        int k0, int k1, int64_t n)
+{
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x)
+    {
+        int i, j, k;
+        plane_shell_cell(b, k0, k1, t, i, j, k);
+        ghost_at<T>(state, prim, b, bg, o, st, i, j, k);
+    }
 }
 
 // Static-metric sources (:255-298) from the floored primitives and, for
@@ -603,61 +628,49 @@ faces_tile(const T *__restrict__ prim, const T *__restrict__ src,
     const bool col_ok = a < kTC && bb < kTC && ci <= b.hi[0] && cj <= b.hi[1];
     const int ci_c = min(ci, b.hi[0]), cj_c = min(cj, b.hi[1]);
 
-    // own-column z window P(k-1..k+2) and the z face below k0
+    // The z march starts two planes below k0: plane k0-2 only computes
+    // the tile geometry of plane k0-1, plane k0-1 only the z face below
+    // k0.  Every plane's geometry and every z face thus come from the same
+    // code as in the rest of the march, so the face below k0 equals the
+    // block below's upper face bit for bit: the RHS does not depend on
+    // where the z blocks start.  w0..w3 is this column's window
+    // P(k-1 .. k+2) of the z face above plane k.
     PVT<T> w0, w1, w2, w3;
     ConsT<T> Flo = zero_cons<T>();
     double macc = 0.0;
-    tile_geometry<T, BGK>(Gb, bg, o, i0, j0, k0, tid);
-    __syncthreads();
-    {
-        w0 = load_pv_global<T, CG>(prim, b.pcs, b.gidx(ci_c, cj_c, k0 - 2));
-        w1 = load_pv_global<T, CG>(prim, b.pcs, b.gidx(ci_c, cj_c, k0 - 1));
-        w2 = load_pv_global<T, CG>(prim, b.pcs, b.gidx(ci_c, cj_c, k0));
-        w3 = load_pv_global<T, CG>(prim, b.pcs, b.gidx(ci_c, cj_c, k0 + 1));
-        if (col_ok)
-        {
-            double x, y, z;
-            cell_xyz(o, ci, cj, k0 - 1, x, y, z);
-            GeoT<T> gl, gr, gf;
-            metric_T<T, false, BGK>(bg, x, y, z, gl, nullptr);
-            geo_load(Gb, nG, (bb + 1) * kGW + (a + 1), gr);
-            average_geo(gl, gr, gf);
-            Flo = face_flux(o, w0, w1, w2, w3, gf, 2);
-            // a box counts the sphere faces whose upper cell it holds, in
-            // every direction, so the boxes of a level count each once
-            if (MDOT && k0 == b.lo[2])
-                macc += mdot_face(o, ci, cj, k0 - 1, 2, gf, Flo.D);
-        }
-        // shift so that w0..w3 = P(k0-1 .. k0+2) after the next load
-        w0 = w1;
-        w1 = w2;
-        w2 = w3;
-    }
+    w0 = load_pv_global<T, CG>(prim, b.pcs, b.gidx(ci_c, cj_c, k0 - 2));
+    w1 = load_pv_global<T, CG>(prim, b.pcs, b.gidx(ci_c, cj_c, k0 - 1));
+    w2 = load_pv_global<T, CG>(prim, b.pcs, b.gidx(ci_c, cj_c, k0));
 
     int cur = 0;
-    for (int k = k0; k <= k1; ++k)
+#pragma unroll 1
+    for (int k = k0 - 2; k <= k1; ++k)
     {
         T *Gc = Gb + cur * kGeoFields * nG;
         T *Gn = Gb + (cur ^ 1) * kGeoFields * nG;
-        w3 = load_pv_global<T, CG>(prim, b.pcs, b.gidx(ci_c, cj_c, k + 2));
+        const bool zface = k >= k0 - 1; // the z face above plane k
+        const bool cells = k >= k0;     // plane k's x/y faces and RHS
+        if (zface)
+            w3 = load_pv_global<T, CG>(prim, b.pcs, b.gidx(ci_c, cj_c, k + 2));
         // primitive cross tile at plane k (clamped to the ghosted box)
-        for (int idx = tid; idx < nP; idx += kTB * kTB)
-        {
-            const int u = idx % kPW, v = idx / kPW;
-            if ((u < 2 || u > kPW - 3) && (v < 2 || v > kPW - 3))
-                continue;
-            const int gi = min(max(i0 - 2 + u, b.glo[0]), b.ghi[0]);
-            const int gj = min(max(j0 - 2 + v, b.glo[1]), b.ghi[1]);
-            const int64_t g = b.gidx(gi, gj, k);
+        if (cells)
+            for (int idx = tid; idx < nP; idx += kTB * kTB)
+            {
+                const int u = idx % kPW, v = idx / kPW;
+                if ((u < 2 || u > kPW - 3) && (v < 2 || v > kPW - 3))
+                    continue;
+                const int gi = min(max(i0 - 2 + u, b.glo[0]), b.ghi[0]);
+                const int gj = min(max(j0 - 2 + v, b.glo[1]), b.ghi[1]);
+                const int64_t g = b.gidx(gi, gj, k);
 #pragma unroll
-            for (int c = 0; c < 5; ++c)
-                P[c * nP + idx] = rdro<CG>(&prim[c * b.pcs + g]);
-        }
+                for (int c = 0; c < 5; ++c)
+                    P[c * nP + idx] = rdro<CG>(&prim[c * b.pcs + g]);
+            }
         tile_geometry<T, BGK>(Gn, bg, o, i0, j0, k + 1, tid);
         __syncthreads();
 
         // x face between cells (i0+a-1, i0+a) in row j0+bb
-        if (bb < kTC && cj <= b.hi[1] && i0 + a - 1 <= b.hi[0])
+        if (cells && bb < kTC && cj <= b.hi[1] && i0 + a - 1 <= b.hi[0])
         {
             const int row = (bb + 2) * kPW;
             GeoT<T> gf;
@@ -676,7 +689,7 @@ faces_tile(const T *__restrict__ prim, const T *__restrict__ src,
             Fx[4 * nFx + fi] = f.tau;
         }
         // y face between rows (j0+bb-1, j0+bb) in column i0+a
-        if (a < kTC && ci <= b.hi[0] && j0 + bb - 1 <= b.hi[1])
+        if (cells && a < kTC && ci <= b.hi[0] && j0 + bb - 1 <= b.hi[1])
         {
             GeoT<T> gf;
             geo_avg_smem(Gc, nG, bb * kGW + a + 1, (bb + 1) * kGW + a + 1, gf);
@@ -697,7 +710,7 @@ faces_tile(const T *__restrict__ prim, const T *__restrict__ src,
         }
         // z face at k+1/2 for this column
         ConsT<T> Fhi = zero_cons<T>();
-        if (col_ok)
+        if (zface && col_ok)
         {
             GeoT<T> gf, gA, gB;
             const int cell = (bb + 1) * kGW + a + 1;
@@ -705,12 +718,14 @@ faces_tile(const T *__restrict__ prim, const T *__restrict__ src,
             geo_load(Gn, nG, cell, gB);
             average_geo(gA, gB, gf);
             Fhi = face_flux(o, w0, w1, w2, w3, gf, 2);
-            if (MDOT && k < b.hi[2])
+            // a box counts the sphere faces whose upper cell it holds, in
+            // every direction, so the boxes of a level count each once
+            if (MDOT && (cells ? k < b.hi[2] : k0 == b.lo[2]))
                 macc += mdot_face(o, ci, cj, k, 2, gf, Fhi.D);
         }
         __syncthreads();
 
-        if (col_ok)
+        if (cells && col_ok)
         {
             const int fxl = bb * kTB + a, fxh = bb * kTB + a + 1;
             const int fyl = a * kTB + bb, fyh = a * kTB + bb + 1;
@@ -737,9 +752,12 @@ faces_tile(const T *__restrict__ prim, const T *__restrict__ src,
                 rhs[c * b.rcs + ri] = out[c];
         }
         Flo = Fhi;
-        w0 = w1;
-        w1 = w2;
-        w2 = w3;
+        if (zface)
+        {
+            w0 = w1;
+            w1 = w2;
+            w2 = w3;
+        }
         cur ^= 1;
         __syncthreads();
     }
@@ -1021,7 +1039,8 @@ stage_item(const double *un, int64_t ucs, const double *us, int64_t tcs,
            T *__restrict__ src, const BoxDev &b, const Background &bg,
            const Options &o, int stage, double dt, bool prep, bool store_p,
            bool cfl, const double inv[3], DevStatus *st, int64_t t,
-           unsigned long long cnt[4], double &cell_inv)
+           unsigned long long cnt[4], double &cell_inv,
+           const T *__restrict__ prim_in = nullptr)
 {
     const double cst = (stage == 2) ? dt : 0.5 * dt;
     const double dt6 = dt / 6.0;
@@ -1082,8 +1101,9 @@ stage_item(const double *un, int64_t ucs, const double *us, int64_t tcs,
             metric_T<T, false, BGK>(bg, x, y, z, f.g, nullptr);
         double gLL[6];
         gLL_double(f.g, gLL);
+        const T *pg = prim_in ? prim_in : prim;
         const double p_guess =
-            (mixed && prim) ? double(rd<CG>(&prim[1 * b.pcs + g])) : 0.0;
+            (mixed && pg) ? double(rd<CG>(&pg[1 * b.pcs + g])) : 0.0;
         // recovery with atmosphere (:60-110)
         Prim pr;
         const bool ok = cell_con2prim(o, c, f.g, p_guess, pr);
@@ -1139,7 +1159,7 @@ stage_item(const double *un, int64_t ucs, const double *us, int64_t tcs,
             if (!okn)
             {
                 record_error(st, cfl && !prep ? 4 : 2,
-                             cfl && !prep ? t : g);
+                             cfl && !prep ? b.t0 + t : g);
                 pn.rho = pn.p = 1.0;
                 pn.v[0] = pn.v[1] = pn.v[2] = 0.0;
                 pn.eps = 1.0;
@@ -1165,7 +1185,7 @@ __global__ void __launch_bounds__(256, kMinBlocks<T>)
             double *__restrict__ acc, T *__restrict__ prim,
             T *__restrict__ src, BoxDev b, Background bg, Options o,
             int stage, double dt, int prep_flag, int cfl, double i0,
-            double i1, double i2, DevStatus *st)
+            double i1, double i2, DevStatus *st, const T *__restrict__ prim_in)
 {
     unsigned long long cnt[4] = {0, 0, 0, 0};
     const int64_t n = b.ivol();
@@ -1183,7 +1203,7 @@ __global__ void __launch_bounds__(256, kMinBlocks<T>)
             stage_item<MODE, T, false, BGK>(un, ucs, us, tcs, out, ocs, kv, acc,
                                             prim, src,
                                 b, bg, o, stage, dt, prep, store_p, cfl != 0,
-                                inv, st, t, cnt, cell_inv);
+                                inv, st, t, cnt, cell_inv, prim_in);
         flush_counts(st, cnt);
         cnt[0] = cnt[1] = cnt[2] = cnt[3] = 0;
         if (cfl)
@@ -1220,7 +1240,7 @@ __device__ __forceinline__ double cfl_item(const double *__restrict__ state,
         Prim pr;
         if (!con2prim(o, load_cons<CG>(state, b.cs, b.gidx(i, j, k)), gUU, pr,
                       nullptr, nullptr))
-            record_error(st, 4, t);
+            record_error(st, 4, b.t0 + t);
         else
             cell = cfl_speed<T>(o, pr, geo, inv);
     }
@@ -1447,7 +1467,9 @@ __global__ void __launch_bounds__(kEnsItemCells, kMinBlocks<T>)
     k_ensemble(EnsLaunch a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ __align__(16) EnsMember ms;
+    // raw storage: the member record is copied in word by word below
+    __shared__ __align__(16) unsigned char ms_raw[sizeof(EnsMember)];
+    EnsMember &ms = *reinterpret_cast<EnsMember *>(ms_raw);
     __shared__ int64_t item_sh;
     const int tid = threadIdx.y * kTB + threadIdx.x;
     EnsControl *ctl = a.ctl;
@@ -2165,6 +2187,18 @@ void launch_fill_ghosts(double *state, T *prim, const BoxDev &b,
 }
 
 template <typename T>
+void launch_fill_ghost_planes(double *state, T *prim, const BoxDev &b,
+                              const Background &bg, const Options &o,
+                              DevStatus *st, int k0, int k1, cudaStream_t s)
+{
+    const int64_t n = plane_shell_count(b, k0, k1);
+    if (n <= 0)
+        return;
+    k_fill_ghost_planes<T><<<grid_for(n, 256), 256, 0, s>>>(state, prim, b, bg,
+                                                           o, st, k0, k1, n);
+}
+
+template <typename T>
 void launch_cells(const double *state, T *prim, T *src, const BoxDev &b,
                   const Background &bg, const Options &o, DevStatus *st,
                   cudaStream_t s)
@@ -2225,7 +2259,7 @@ void launch_stage(int mode, const double *un, int64_t ucs, const double *us,
                   double *acc, T *prim, T *src, int prep, const BoxDev &b,
                   const Background &bg, const Options &o, int stage,
                   double dt, bool cfl, const double inv_dx[3], DevStatus *st,
-                  cudaStream_t s)
+                  cudaStream_t s, const T *prim_in)
 {
     const int grid = grid_for(b.ivol(), 256);
     const double i0 = inv_dx ? inv_dx[0] : 0.0, i1 = inv_dx ? inv_dx[1] : 0.0,
@@ -2233,7 +2267,8 @@ void launch_stage(int mode, const double *un, int64_t ucs, const double *us,
     const int pf = prep, cf = cfl ? 1 : 0;
     auto go = [&](auto kern) {
         kern<<<grid, 256, 0, s>>>(un, ucs, us, tcs, out, ocs, k, acc, prim, src,
-                                  b, bg, o, stage, dt, pf, cf, i0, i1, i2, st);
+                                  b, bg, o, stage, dt, pf, cf, i0, i1, i2, st,
+                                  prim_in);
     };
     // one instantiation per background kind (only its own metric code)
     const bool pn = bg.kind == 1;
@@ -2346,6 +2381,9 @@ void launch_ccz4_probe(const double *s, const BoxDev &b, const Options &o,
     template void launch_fill_ghosts<T>(double *, T *, const BoxDev &,        \
                                         const Background &, const Options &,  \
                                         DevStatus *, cudaStream_t);           \
+    template void launch_fill_ghost_planes<T>(                                \
+        double *, T *, const BoxDev &, const Background &, const Options &,   \
+        DevStatus *, int, int, cudaStream_t);                                 \
     template void launch_cells<T>(const double *, T *, T *, const BoxDev &,   \
                                   const Background &, const Options &,        \
                                   DevStatus *, cudaStream_t);                 \
@@ -2358,7 +2396,8 @@ void launch_ccz4_probe(const double *s, const BoxDev &b, const Options &o,
                                   const T *, double *, T *, T *, int,         \
                                   const BoxDev &, const Background &,         \
                                   const Options &, int, double, bool,         \
-                                  const double *, DevStatus *, cudaStream_t);
+                                  const double *, DevStatus *, cudaStream_t,  \
+                                  const T *);
 
 GRHD_INSTANTIATE(double)
 GRHD_INSTANTIATE(float)

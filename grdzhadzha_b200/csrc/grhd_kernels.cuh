@@ -18,6 +18,11 @@ struct BoxDev
     int64_t cs;  // state component stride
     int64_t rcs; // interior array component stride
     int64_t pcs; // primitive cache component stride (ghosted volume)
+    // interior index, within the box it views, of this box's first
+    // interior cell: 0 for a whole box; a z range of planes of a box (the
+    // same ghosted layout and strides, its own lo/hi/in in z) starts at
+    // the index of its first plane
+    int64_t t0 = 0;
 
     __host__ __device__ int64_t gidx(int i, int j, int k) const
     {
@@ -40,6 +45,63 @@ struct BoxDev
         return (int64_t)in[0] * in[1] * in[2];
     }
 };
+
+// The cells of the ghosted planes k0..k1 of box b that lie outside its
+// interior: whole planes below lo[2] and above hi[2], and the ring
+// "ghosted plane minus interior plane" of the planes in between.  Cell t
+// of that set in plane order (x fastest; in a ring the rows outside the
+// interior first, then the x margins of the interior rows).
+__host__ __device__ inline int64_t plane_shell_count(const BoxDev &b, int k0,
+                                                     int k1)
+{
+    const int64_t P = (int64_t)b.gn[0] * b.gn[1];
+    const int64_t R = P - (int64_t)b.in[0] * b.in[1];
+    const int nb = max(0, min(k1, b.lo[2] - 1) - k0 + 1);
+    const int nm = max(0, min(k1, b.hi[2]) - max(k0, b.lo[2]) + 1);
+    const int nt = max(0, k1 - max(k0, b.hi[2] + 1) + 1);
+    return (int64_t)(nb + nt) * P + (int64_t)nm * R;
+}
+
+__host__ __device__ inline void plane_shell_cell(const BoxDev &b, int k0,
+                                                 int k1, int64_t t, int &i,
+                                                 int &j, int &k)
+{
+    const int64_t gx = b.gn[0];
+    const int64_t P = gx * b.gn[1];
+    const int64_t R = P - (int64_t)b.in[0] * b.in[1];
+    const int nb = max(0, min(k1, b.lo[2] - 1) - k0 + 1);
+    const int nm = max(0, min(k1, b.hi[2]) - max(k0, b.lo[2]) + 1);
+    const int64_t n1 = (int64_t)nb * P, n2 = (int64_t)nm * R;
+    if (t < n1 || t >= n1 + n2)
+    {
+        // a whole ghost plane below or above the interior
+        const int kb = t < n1 ? k0 : max(k0, b.hi[2] + 1);
+        const int64_t u = t < n1 ? t : t - n1 - n2;
+        k = kb + (int)(u / P);
+        const int64_t r = u % P;
+        j = b.glo[1] + (int)(r / gx);
+        i = b.glo[0] + (int)(r % gx);
+        return;
+    }
+    const int64_t u = t - n1;
+    k = max(k0, b.lo[2]) + (int)(u / R);
+    int64_t r = u % R;
+    const int64_t ylo = b.lo[1] - b.glo[1];
+    const int64_t ny_out = b.gn[1] - b.in[1];
+    if (r < ny_out * gx)
+    {
+        const int64_t jj = r / gx;
+        j = (jj < ylo) ? b.glo[1] + (int)jj : b.hi[1] + 1 + (int)(jj - ylo);
+        i = b.glo[0] + (int)(r % gx);
+        return;
+    }
+    r -= ny_out * gx;
+    const int64_t xlo = b.lo[0] - b.glo[0];
+    const int64_t nx_out = b.gn[0] - b.in[0];
+    j = b.lo[1] + (int)(r / nx_out);
+    const int64_t ii = r % nx_out;
+    i = (ii < xlo) ? b.glo[0] + (int)ii : b.hi[0] + 1 + (int)(ii - xlo);
+}
 
 // Device-side status of one call: the first recovery failure in the
 // reference's iteration order (key = where << 56 | linear index), the
@@ -86,6 +148,12 @@ template <typename T>
 void launch_fill_ghosts(double *state, T *prim, const BoxDev &b,
                         const Background &bg, const Options &o, DevStatus *st,
                         cudaStream_t s);
+// The same fill restricted to the ghosted planes k0..k1 (their cells
+// outside the interior).
+template <typename T>
+void launch_fill_ghost_planes(double *state, T *prim, const BoxDev &b,
+                              const Background &bg, const Options &o,
+                              DevStatus *st, int k0, int k1, cudaStream_t s);
 // Interior con2prim into the primitive cache + sources.
 template <typename T>
 void launch_cells(const double *state, T *prim, T *src, const BoxDev &b,
@@ -112,15 +180,15 @@ void launch_recover(double *state, const BoxDev &b, const Background &bg,
 // Integrator stage fused with the post-update recovery; mode 0 RK4 stage
 // `stage`, 1 Euler update, 2 SSPRK2 combine.  With prep the stage also
 // prepares the next RHS (primitive cache and sources); the mixed path
-// reads its con2prim start from `prim` either way.  With cfl it
-// accumulates the next max inverse dt into st->maxinv_bits.
+// reads its con2prim start from `prim_in` (`prim` when null) either way.
+// With cfl it accumulates the next max inverse dt into st->maxinv_bits.
 template <typename T>
 void launch_stage(int mode, const double *un, int64_t ucs, const double *us,
                   int64_t tcs, double *out, int64_t ocs, const T *k,
                   double *acc, T *prim, T *src, int prep, const BoxDev &b,
                   const Background &bg, const Options &o, int stage,
                   double dt, bool cfl, const double inv_dx[3], DevStatus *st,
-                  cudaStream_t s);
+                  cudaStream_t s, const T *prim_in = nullptr);
 // The CFL speed in the FP64 metric and arithmetic, or (mixed) in those of
 // the mixed path's fused stage.
 void launch_max_inv_dt(const double *state, const BoxDev &b,

@@ -413,11 +413,13 @@ def advance_ssprk2(p, box, state, time, dt) -> Diag:
     return d
 
 
-def advance_rk4(p, box, state, time, dt) -> Diag:
+def advance_rk4(p, box, state, time, dt, L=None) -> Diag:
+    """One RK4 step of the oracle (L: the build, default the checker)."""
     d, err = Diag(), Error()
     inv = np.array([1.0 / p.dx] * 3)
-    st = lib().orc_advance_rk4(C.byref(p), C.byref(box), _dp(state), _dp(inv),
-                               time, dt, C.byref(d), C.byref(err))
+    st = (L or lib()).orc_advance_rk4(C.byref(p), C.byref(box), _dp(state),
+                                      _dp(inv), time, dt, C.byref(d),
+                                      C.byref(err))
     if st:
         raise OracleError(st, err)
     return d

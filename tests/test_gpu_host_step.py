@@ -5,7 +5,11 @@ conserved components, the primitives of the z planes holding excised
 cells, the pressure in mixed precision), so the test poisons every other
 primitive slot of the host state with NaN: the results must still equal
 the device call's bit for bit (both run the same kernels on the same
-inputs), in FP64 and in mixed precision, over two steps."""
+inputs), in FP64 and in mixed precision, over three steps.  The first
+call computes the CFL speed and runs copy in, step, copy out in turn;
+the later calls are given it and run the step as a wavefront over z
+chunks of 8 planes with the copies overlapped (3, 4 and 4 chunks here,
+the last one short for 30 planes)."""
 import numpy as np
 import pytest
 
@@ -28,9 +32,12 @@ def _excised_planes(p, box):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-@pytest.mark.parametrize("name", ["torus_a09", "michel_c1"])
+@pytest.mark.parametrize("name", ["torus_a09", "torus_a09_n30", "michel_c1"])
 def test_host_step_equals_device_step(name, precision):
-    p, box, s, t = cases.CASES[name]()
+    if name == "torus_a09_n30":
+        p, box, s, t = cases.torus_a09(n=30)
+    else:
+        p, box, s, t = cases.CASES[name]()
     assert p.excision_radius > 0.0
     op = cases.gpu_operator(p, precision=precision)
     lv = cases.gpu_level(box, s)
@@ -44,7 +51,7 @@ def test_host_step_equals_device_step(name, precision):
         poisoned[keep] = V[c][keep]
         V[c] = poisoned
     mi_d = mi_h = 0.0
-    for _ in range(2):
+    for _ in range(3):
         dt_d, mi_d, d_d = op.advance_rk4_cfl(lv, 0.25, time=t,
                                              max_inverse_dt=mi_d)
         dt_h, mi_h, d_h, hb, db = op.advance_rk4_cfl_host(
