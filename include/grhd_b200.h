@@ -293,7 +293,14 @@ int grhd_advance_rk4_cfl_steps(grhd_ctx *ctx, double *state,
  * grhd_advance_rk4_cfl, same results bit for bit) and copies all 11
  * components back; the other primitive components on input are ignored.
  * h2d_bytes / d2h_bytes (may be NULL) receive the bytes moved each way.
- * The device copy of the state lives in the context.  Synchronous. */
+ * The device copy of the state lives in the context.  Synchronous.
+ * With *max_inverse_dt > 0 (the previous call's value) and no accretion
+ * sphere, the step runs as a wavefront over z chunks of the box on the
+ * given stream and two streams of the context, copies in and out
+ * overlapping the computation; otherwise the state is copied in, stepped
+ * and copied back in turn.  On a recovery failure every copy has finished
+ * when the call returns; in the wavefront the chunks already copied back
+ * then hold the new state. */
 int grhd_advance_rk4_cfl_host(grhd_ctx *ctx, double *host_state,
                               int64_t state_comp_stride,
                               const grhd_box *box,
