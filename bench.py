@@ -462,20 +462,32 @@ def run_adjoint(n, steps, every, fd_steps, hbm_peak):
 
 
 class CpuBaseline:
-    """The reference's algorithm on the host cores: the oracle's timing
-    build (oracle/liborc_grhd_fast.so, -O3 with AVX2 + FMA; the parity
-    checker is the no-contraction build of the same source) on a bounded
-    sample of the same workload -- the central 128 x 128 columns of the
-    256^3 torus grid over nz = min(256, 16 x threads) mid-plane z planes,
-    as one box whose RHS runs as z-slab boxes of at least 16 planes, one
-    thread each (the reference's per-box loops, its MPI ranks standing as
-    threads).  One sample is one complete step as the GPU arm's: the CFL
-    bound of the current state, then one RK4 step (4 RHS evaluations, the
-    stage combinations, the post-stage recoveries).  The sample's state is
-    built by the oracle (torus + numpy-seeded 1e-3 perturbation +
-    recovery)."""
+    """The reference's algorithm on the host cores, on a bounded sample of
+    the same workload: the central 128 x 128 columns of the 256^3 torus
+    grid over nz mid-plane z planes, as one box stepped as z-slab boxes,
+    one thread each (the reference's per-box loops, its MPI ranks standing
+    as threads).  One sample is one complete step as the GPU arm's: the
+    CFL bound of the current state, then one RK4 step (4 RHS evaluations,
+    the stage combinations, the post-stage recoveries).
 
-    BUILD = "gcc -O3 -march=x86-64-v3 -ffp-contract=fast"
+    kind "reference" (where oracle/_ref was built): GRDzhadzha's own
+    operator, its headers compiled unmodified at -O3 -march=x86-64-v3
+    against oracle/shim (oracle/ref_capi.cpp: the RK4 step from the
+    operator's compute_rhs and update_conserved, slab ghosts exchanged
+    between the RHS evaluations, slabs of 8 planes).  The reference has no
+    excision: the sample runs without it (the cells inside the horizon
+    near the hole then fail their recovery and are reset to the
+    atmosphere, as the reference does).
+    kind "port" (otherwise): the oracle's timing build
+    (oracle/liborc_grhd_fast.so, -O3 with AVX2 + FMA), slabs of 16 planes,
+    with the workload's excision.
+
+    The sample's state is built by the oracle (torus + numpy-seeded 1e-3
+    perturbation + recovery)."""
+
+    PORT_BUILD = "gcc -O3 -march=x86-64-v3 -ffp-contract=fast"
+    REF_BUILD = ("g++ -O3 -march=x86-64-v3 (GRDzhadzha's headers, "
+                 "unmodified, against oracle/shim)")
 
     def __init__(self, threads):
         import ctypes as C
@@ -485,6 +497,10 @@ class CpuBaseline:
 
         self.O, self.C = O, C
         self.threads = threads
+        self.kind = "reference" if O.have_ref() else "port"
+        self.build = self.REF_BUILD if self.kind == "reference" \
+            else self.PORT_BUILD
+        planes = 8 if self.kind == "reference" else 16
         O.set_threads(threads)
         n = N_CELLS
         dx = 2.0 * HALF_WIDTH / n
@@ -496,9 +512,10 @@ class CpuBaseline:
                              atmo_max_velocity_squared=0.8,
                              rec_max_iterations=80,
                              rec_max_velocity_squared=0.9, limiter_theta=2.0,
-                             excision_radius=1.5)
+                             excision_radius=(0.0 if self.kind == "reference"
+                                              else 1.5))
         nxy = 128
-        nz = min(n, 16 * threads)
+        nz = min(n, planes * threads)
         box = O.Box()
         x0, z0 = n // 2 - nxy // 2, n // 2 - nz // 2
         for d, (lo, hi) in enumerate(((x0, x0 + nxy - 1),
@@ -521,22 +538,37 @@ class CpuBaseline:
         O.fill_conserved_from_primitives(p, box, s)
         O.recover_primitives(p, box, s)
         O.set_threads(1)
-        self.L = O.fast_lib()
-        self.L.orc_set_threads(threads)
+        self.ranks = min(threads, nz // 2)
+        if self.kind == "port":
+            self.L = O.fast_lib()
+            self.L.orc_set_threads(threads)
         self.p, self.box, self.s = p, box, s
         self.inv = np.array([1.0 / dx] * 3)
         self.t = 0.0
         self.cells = nxy * nxy * nz
+        what = ("GRDzhadzha's own operator" if self.kind == "reference"
+                else "the oracle's timing build")
         self.desc = (f"one RK4 step with its CFL bound (4 RHS evaluations, "
-                     f"stage combinations, post-stage recoveries) of the "
-                     f"oracle's timing build ({self.BUILD}; the reference's "
-                     f"per-box algorithm, z-slab boxes of "
-                     f"{nz // threads}+ planes, one thread each) over the "
-                     f"central {nxy}x{nxy}x{nz} cells of the {n}^3 grid")
+                     f"stage combinations, post-stage recoveries) of "
+                     f"{what} ({self.build}; z-slab boxes of "
+                     f"{nz // self.ranks}+ planes, one thread each"
+                     + ("; no excision: the reference has none"
+                        if self.kind == "reference" else "")
+                     + f") over the central {nxy}x{nxy}x{nz} cells of the "
+                     f"{n}^3 grid")
 
     def sample(self):
         """(cell-updates/s, seconds) of one step of the sample."""
-        O, C, L = self.O, self.C, self.L
+        O, C = self.O, self.C
+        if self.kind == "reference":
+            t0 = time.perf_counter()
+            dt, _, _ = O.ref_advance_rk4_cfl(self.p, self.box, self.s,
+                                             self.t, CFL, ranks=self.ranks,
+                                             fast=True)
+            el = time.perf_counter() - t0
+            self.t += dt
+            return self.cells / el, el
+        L = self.L
         err = O.Error()
         diag = O.Diag()
         mi = C.c_double()
@@ -760,8 +792,8 @@ def main():
             "dtype": "f64", "data": "synthetic",
             "config": workload_config(N_CELLS),
             "cpu_baseline": {"value": value, "unit": "cell-updates/s",
-                             "cores": threads, "kind": "port",
-                             "build": CpuBaseline.BUILD,
+                             "cores": threads, "kind": cb.kind,
+                             "build": cb.build,
                              "sample": cb.desc,
                              "cells_per_step": cb.cells},
             "e2e": {"value": value, "unit": "cell-updates/s",
@@ -843,7 +875,7 @@ def main():
         cb.sample()
         rate = max(cb.sample()[0] for _ in range(2))
         cpu = {"value": rate, "unit": "cell-updates/s", "cores": threads,
-               "kind": "port", "build": CpuBaseline.BUILD,
+               "kind": cb.kind, "build": cb.build,
                "sample": cb.desc, "cells_per_step": cb.cells}
     if rank == 0:
         line = {

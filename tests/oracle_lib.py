@@ -21,6 +21,13 @@ _LIB_PATH = os.path.join(_ORACLE_DIR, "liborc_grhd.so")
 # the same source built for timing (-O3, FMA contraction allowed)
 _FAST_LIB_PATH = os.path.join(_ORACLE_DIR, "liborc_grhd_fast.so")
 
+# GRDzhadzha's own operator (its headers compiled unmodified against
+# oracle/shim, oracle/ref_capi.cpp): present where the reference tree was
+# available to build it (make -C oracle ref)
+REF_DIR = os.path.join(_ORACLE_DIR, "_ref")
+_REF_LIB_PATH = os.path.join(REF_DIR, "libref_grhd.so")
+_REF_FAST_LIB_PATH = os.path.join(REF_DIR, "libref_grhd_fast.so")
+
 NCOMP = 11
 D, S1, S2, S3, TAU, RHO, EPS, PRESS, V1, V2, V3 = range(11)
 BG_KERR_SCHILD, BG_BINARY_PN = 0, 1
@@ -171,6 +178,100 @@ def fast_lib():
             build()
         _fast_lib = _bind(C.CDLL(_FAST_LIB_PATH))
     return _fast_lib
+
+
+_ref_libs = {}
+
+
+def have_ref() -> bool:
+    """Whether the reference's own operator library was built."""
+    return os.path.exists(_REF_LIB_PATH)
+
+
+def ref_lib(fast=False):
+    """The reference's own operator behind the oracle's C interface
+    (`ref_` entry points): the parity build, or (fast) the -O3 build timed
+    as the CPU baseline's reference implementation."""
+    path = _REF_FAST_LIB_PATH if fast else _REF_LIB_PATH
+    if path not in _ref_libs:
+        L = C.CDLL(path)
+        P, B = C.POINTER(Params), C.POINTER(Box)
+        dp, i64 = C.POINTER(C.c_double), C.c_int64
+        E, Dg = C.POINTER(Error), C.POINTER(Diag)
+        L.ref_compute_rhs.argtypes = [P, B, dp, dp, i64, dp, C.c_double, E]
+        L.ref_recover_primitives.argtypes = [P, B, dp, C.c_double, Dg]
+        L.ref_compute_max_inverse_dt.argtypes = [P, B, dp, dp, C.c_double,
+                                                 dp, E]
+        L.ref_update_conserved.argtypes = [P, B, dp, dp, i64, C.c_double,
+                                           C.c_double, C.c_int, Dg]
+        L.ref_advance_ssprk2.argtypes = [P, B, dp, dp, C.c_double,
+                                         C.c_double, Dg, E]
+        L.ref_advance_rk4_cfl_ranks.argtypes = [
+            P, B, dp, dp, C.c_double, C.c_double, C.c_double, C.c_int, dp,
+            dp, Dg, E]
+        L.ref_ccz4_compute_rhs.argtypes = [P, B, dp, dp, i64, dp, E]
+        L.ref_ccz4_recover_primitives.argtypes = [P, B, dp, Dg]
+        L.ref_ccz4_compute_max_inverse_dt.argtypes = [P, B, dp, dp, dp, E]
+        _ref_libs[path] = L
+    return _ref_libs[path]
+
+
+def ref_compute_rhs(p, box, state, time=0.0):
+    n = interior_cells(box)
+    rhs = np.zeros(5 * n, dtype=np.float64)
+    inv = np.array([1.0 / p.dx] * 3)
+    err = Error()
+    st = ref_lib().ref_compute_rhs(C.byref(p), C.byref(box), _dp(state),
+                                   _dp(rhs), n, _dp(inv), time,
+                                   C.byref(err))
+    if st:
+        raise OracleError(st, err)
+    return rhs
+
+
+def ref_recover_primitives(p, box, state, time=0.0) -> Diag:
+    d = Diag()
+    st = ref_lib().ref_recover_primitives(C.byref(p), C.byref(box),
+                                          _dp(state), time, C.byref(d))
+    if st:
+        raise OracleError(st)
+    return d
+
+
+def ref_max_inverse_dt(p, box, state, time=0.0):
+    out = C.c_double()
+    inv = np.array([1.0 / p.dx] * 3)
+    err = Error()
+    st = ref_lib().ref_compute_max_inverse_dt(C.byref(p), C.byref(box),
+                                              _dp(state), _dp(inv), time,
+                                              C.byref(out), C.byref(err))
+    if st:
+        raise OracleError(st, err)
+    return out.value
+
+
+def ref_advance_ssprk2(p, box, state, time, dt) -> None:
+    d, err = Diag(), Error()
+    inv = np.array([1.0 / p.dx] * 3)
+    st = ref_lib().ref_advance_ssprk2(C.byref(p), C.byref(box), _dp(state),
+                                      _dp(inv), time, dt, C.byref(d),
+                                      C.byref(err))
+    if st:
+        raise OracleError(st, err)
+
+
+def ref_advance_rk4_cfl(p, box, state, time, cfl, ranks=1, fast=False):
+    """(dt, max inverse dt of the input, diag) of one CFL-limited RK4 step
+    built from the reference operator's methods, one z slab per thread."""
+    d, err = Diag(), Error()
+    mi, dt = C.c_double(), C.c_double()
+    inv = np.array([1.0 / p.dx] * 3)
+    st = ref_lib(fast).ref_advance_rk4_cfl_ranks(
+        C.byref(p), C.byref(box), _dp(state), _dp(inv), time, cfl, 0.0,
+        ranks, C.byref(mi), C.byref(dt), C.byref(d), C.byref(err))
+    if st:
+        raise OracleError(st, err)
+    return dt.value, mi.value, d
 
 
 def _bind(L):
