@@ -216,6 +216,25 @@ def ref_lib(fast=False):
     return _ref_libs[path]
 
 
+def ref_kitp_lib():
+    """The reference KITP disk driver's functions (oracle/ref_kitp.cpp)."""
+    path = os.path.join(REF_DIR, "libref_kitp.so")
+    if path not in _ref_libs:
+        L = C.CDLL(path)
+        P, B = C.POINTER(Params), C.POINTER(Box)
+        dp, i64 = C.POINTER(C.c_double), C.c_int64
+        KC, KD = C.POINTER(KitpConfig), C.POINTER(KitpDisk)
+        L.ref_kitp_fill.argtypes = [P, KD, B, dp, C.c_double]
+        L.ref_kitp_source_rhs.argtypes = [P, KC, B, dp, dp, i64, C.c_double,
+                                          C.c_int]
+        L.ref_kitp_sink_decay.argtypes = [P, KC, B, dp, C.c_double,
+                                          C.c_double]
+        L.ref_kitp_advance_ssprk2.argtypes = [P, KC, B, dp, C.c_double,
+                                              C.c_double, C.POINTER(Error)]
+        _ref_libs[path] = L
+    return _ref_libs[path]
+
+
 def ref_compute_rhs(p, box, state, time=0.0):
     n = interior_cells(box)
     rhs = np.zeros(5 * n, dtype=np.float64)

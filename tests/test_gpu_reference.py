@@ -7,7 +7,14 @@ tests/test_oracle_reference.py): one RHS evaluation per conserved component
 max|gpu - ref| / max|ref| <= 1e-12 (Tests/GRHDFixedBGTest/
 GRHDFixedBGTest.cpp:419-421), the physical ghost fill to 1e-13, one SSPRK2
 step's increment to 1e-11 and its conserved state to 1e-13 of scale.  The
-reference has no excision; the fixtures that use it run without it."""
+reference has no excision; the fixtures that use it run without it.
+
+Also the KITP disk driver itself (oracle/_ref/GRHDLevelDataBinaryPNKITPDisk,
+run here): the product reads its KITPCHK1 checkpoint and writes the same
+bytes back, and the device's driver step from its first checkpoint meets
+its second."""
+import os
+
 import numpy as np
 import pytest
 
@@ -63,5 +70,69 @@ def test_ssprk2_step_matches_reference(name):
                         want[:5] - O.interior(box, s))
     full = cases.rel_err(got[:5], want[:5])
     print(f"{name}: SSPRK2 increment {inc}, state {full}")
+    assert np.all(inc <= 1e-11), inc
+    assert np.all(full <= 1e-13), full
+
+
+# ---- the KITP disk driver's own run on the device ----
+
+def _kitp_case(tmp_path):
+    import test_oracle_reference as TR
+    if not os.path.exists(os.path.join(O.REF_DIR, TR.KITP_DRIVER)):
+        pytest.skip("reference KITP driver not built")
+    paths = TR.run_kitp_driver(tmp_path)
+    p = TR.kitp_driver_params()
+    box = O.make_box((TR.KITP_N, TR.KITP_N, TR.KITP_NZ))
+    return TR, paths, p, box
+
+
+def test_reference_checkpoint_round_trips_through_the_device(tmp_path):
+    """The product reads the checkpoint the reference driver wrote (header,
+    signature and the GRHD components of every stored cell, bit for bit)
+    and writes the same state back as the same bytes."""
+    import kitp_checkpoint as KC
+    from grdzhadzha_b200 import io
+    TR, paths, p, box = _kitp_case(tmp_path)
+    h, sig, v = KC.read(paths[1])
+    lv = cases.gpu_level(box, O.new_state(box))
+    hdr = io.read_checkpoint(paths[1], lv, expected_signature=sig)
+    assert (hdr.steps, hdr.time, list(hdr.recovery_totals)) == \
+        (h["steps"], h["time"], h["recovery_totals"])
+    assert np.array_equal(np.moveaxis(lv.state.cpu().numpy(), 0, -1),
+                          v[..., 25:36])
+    out = str(tmp_path / "rewritten.bin")
+    io.write_checkpoint(out, lv, hdr, sig)
+    assert open(out, "rb").read() == open(paths[1], "rb").read()
+
+
+def test_kitp_driver_step_on_the_device_matches_the_reference(tmp_path):
+    """From the reference driver's first checkpoint, the driver's next step
+    on the device (recovery, stable dt, grhd_kitp_advance_ssprk2, recovery)
+    against its second checkpoint: the step's change of the conserved
+    state within 1e-11 of its scale and the state within 1e-13 (the
+    tolerance of the operator's own step parity tests)."""
+    import kitp_checkpoint as KC
+    from grdzhadzha_b200 import io
+    from grdzhadzha_b200.operator import kitp_config
+    TR, paths, p, box = _kitp_case(tmp_path)
+    op = cases.gpu_operator(p)
+    lv = cases.gpu_level(box, O.new_state(box))
+    h1 = io.read_checkpoint(paths[0], lv)
+    start = lv.interior(slice(0, 5)).cpu().numpy()
+    t = h1.time
+    op.recover_primitives(lv, time=t)
+    stable = 0.14 / op.compute_max_inverse_dt(lv, time=t)
+    dt = min(stable, 0.02, 0.06 - t, 0.5 - t, h1.next_checkpoint_time - t)
+    op.kitp_advance_ssprk2(lv, t, dt, kitp_config())
+    op.recover_primitives(lv, time=t + dt)
+    h2, sig, v = KC.read(paths[1])
+    assert t + dt == h2["time"]
+    want = np.moveaxis(v[2:-2, 2:-2, 2:-2, 25:30], -1, 0)
+    got = lv.interior(slice(0, 5)).cpu().numpy()
+    inc = cases.rel_err((got - start).reshape(5, -1),
+                        (want - start).reshape(5, -1))
+    full = cases.rel_err(got.reshape(5, -1), want.reshape(5, -1))
+    print("KITP driver step, device vs reference: increment", inc,
+          "state", full)
     assert np.all(inc <= 1e-11), inc
     assert np.all(full <= 1e-13), full

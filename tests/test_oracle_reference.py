@@ -250,3 +250,123 @@ def test_reference_rk4_ranks_and_oracle_rk4():
                         O.interior(box, b).reshape(5, -1))
     print("reference RK4 vs oracle RK4:", err)
     assert np.all(err <= 1e-14), err
+
+
+# ---- the KITP disk driver (Examples/GRHDLevelDataBinaryPNKITPDisk) ----
+
+KITP_DRIVER = "GRHDLevelDataBinaryPNKITPDisk"
+KITP_N, KITP_NZ, KITP_L = 24, 8, 36.0
+
+
+def kitp_driver_params():
+    """The driver's operator on its 24^2 x 8 grid over 36 M
+    (make_center, make_background_params, make_atmosphere_options,
+    make_recovery_options, :298-346; IdealGasEOS 5/3, :1686)."""
+    dx = KITP_L / KITP_N
+    return O.default_params(
+        background=O.BG_BINARY_PN, pn_mass_1=0.5, pn_mass_2=0.5,
+        pn_separation=8.0, pn_softening_radius=0.5, gamma=5 / 3, dx=dx,
+        center=(0.5 * KITP_N * dx, 0.5 * KITP_N * dx, 0.5 * KITP_NZ * dx),
+        atmo_rho_floor=1e-10, atmo_pressure_floor=8e-14,
+        atmo_max_velocity_squared=0.72, rec_max_velocity_squared=0.75,
+        rec_max_iterations=80, rec_pressure_floor=8e-14, limiter_theta=1.3,
+        use_metric_volume_time_sources=1)
+
+
+def kitp_driver_disk():
+    return O.kitp_disk(mach=10.0, aspect_ratio=0.1, cavity_radius_factor=2.5,
+                       cavity_delta=1e-5, outer_cutoff_radius=1e10,
+                       rho_peak=4e-5)
+
+
+def run_kitp_driver(out_dir):
+    """The reference driver to t = 0.06 with checkpoints every 0.02 (three
+    steps of dt = 0.02, checkpoints after steps 1 and 2)."""
+    rc, out = _run(KITP_DRIVER, "0.06", "--num-cells", str(KITP_N),
+                   "--num-z-cells", str(KITP_NZ), "--domain-length",
+                   str(KITP_L), "--no-frames", "--output-dir", str(out_dir),
+                   "--checkpoint-interval", "0.02", cwd=out_dir)
+    assert rc == 0, out
+    return [os.path.join(out_dir, "checkpoints",
+                         f"checkpoint_step_{n:08d}.bin") for n in (1, 2)]
+
+
+def test_kitp_pieces_equal_reference_driver():
+    """kitp_primitive's disk fill (:398-565), the alpha-viscosity RHS
+    (:676-806), the sink RHS (:567-610, sinks 20 M wide so that they reach
+    the disk) and the sink decay (:612-662): the oracle's restatements
+    equal the driver's own functions bit for bit."""
+    C = O.C
+    L = O.ref_kitp_lib()
+    p = kitp_driver_params()
+    box = O.make_box((KITP_N, KITP_N, KITP_NZ))
+    disk = kitp_driver_disk()
+    k = O.kitp_config(sink_size=20.0, sink_rate=1.0, viscosity_beta=0.2)
+    n = O.interior_cells(box)
+    for t in (0.0, 0.37):
+        a, b = O.new_state(box), O.new_state(box)
+        O.fill_kitp_disk(p, disk, box, a, t)
+        assert L.ref_kitp_fill(C.byref(p), C.byref(disk), C.byref(box),
+                               O._dp(b), t) == 0
+        assert np.array_equal(O.interior(box, a, slice(0, 11)),
+                              O.interior(box, b, slice(0, 11)))
+        O.recover_primitives(p, box, a, t)
+        for which, fn in ((0, O.kitp_viscous_rhs), (1, O.kitp_sink_rhs)):
+            r_o, r_r = np.zeros(5 * n), np.zeros(5 * n)
+            fn(p, k, box, a, r_o, t)
+            L.ref_kitp_source_rhs(C.byref(p), C.byref(k), C.byref(box),
+                                  O._dp(a.copy()), O._dp(r_r), n, t, which)
+            assert np.abs(r_r).max() > 0
+            assert np.array_equal(r_o, r_r), (which, np.abs(r_o - r_r).max())
+        s_o, s_r = a.copy(), a.copy()
+        O.kitp_sink_decay(p, k, box, s_o, t, 0.01)
+        L.ref_kitp_sink_decay(C.byref(p), C.byref(k), C.byref(box),
+                              O._dp(s_r), t, 0.01)
+        assert np.array_equal(O.interior(box, s_o, slice(0, 11)),
+                              O.interior(box, s_r, slice(0, 11)))
+
+
+def kitp_oracle_step(p, k, box, s, t, dt):
+    """advance_kitp_ssprk2 (:842-876) from the oracle's pieces."""
+    old, stage = s.copy(), s.copy()
+    r0 = O.compute_rhs(p, box, s, t)
+    O.kitp_viscous_rhs(p, k, box, s, r0, t)
+    O.update_conserved(p, box, stage, r0, dt, t + dt, True)
+    r1 = O.compute_rhs(p, box, stage, t + dt)
+    O.kitp_viscous_rhs(p, k, box, stage, r1, t + dt)
+    cur = O.interior(box, s)
+    cur[...] = 0.5 * (O.interior(box, old) + O.interior(box, stage)
+                      + dt * r1.reshape(cur.shape))
+    O.kitp_sink_decay(p, k, box, s, t + 0.5 * dt, dt)
+    O.recover_primitives(p, box, s, t + dt)
+
+
+def test_kitp_driver_run_equals_oracle_replay(tmp_path):
+    """The driver's run (:1735-1905: initial fill and recovery; per step a
+    recovery, the stable dt, advance_kitp_ssprk2, a recovery) replayed by
+    the oracle: the GRHD components of both checkpoints equal it bit for
+    bit, and the product's config_signature is the driver's."""
+    import kitp_checkpoint as KC
+    from grdzhadzha_b200 import io
+    paths = run_kitp_driver(tmp_path)
+    p = kitp_driver_params()
+    k = O.kitp_config()
+    box = O.make_box((KITP_N, KITP_N, KITP_NZ))
+    s = O.new_state(box)
+    O.fill_kitp_disk(p, kitp_driver_disk(), box, s, 0.0)
+    O.recover_primitives(p, box, s, 0.0)
+    t, next_ckpt = 0.0, 0.02
+    for n, path in enumerate(paths, start=1):
+        O.recover_primitives(p, box, s, t)
+        stable = 0.14 / max(O.max_inverse_dt(p, box, s, t), 1e-14)
+        dt = min(stable, 0.02, 0.06 - t, 0.5 - t, next_ckpt - t)
+        kitp_oracle_step(p, k, box, s, t, dt)
+        t += dt
+        next_ckpt += 0.02
+        O.recover_primitives(p, box, s, t)
+        h, sig, v = KC.read(path)
+        assert (h["steps"], h["time"]) == (n, t)
+        want = np.moveaxis(v[2:-2, 2:-2, 2:-2, 25:36], -1, 0)
+        assert np.array_equal(O.interior(box, s, slice(0, 11)), want), n
+        assert sig == io.config_signature(
+            num_cells=KITP_N, num_z_cells=KITP_NZ, domain_length=KITP_L)
