@@ -325,9 +325,9 @@ void forward_step(grhd_adjoint *a, grhd_adjoint::Slot &sl, double *next,
         launch_cells<double>(U, sl.P[st], a->src, b, a->bg, a->o, a->status,
                              s);
         launch_faces<double>(sl.P[st], a->src, a->kbuf, b, a->bg, a->o,
-                             a->inv_dx, 32, a->mdot_part, s);
+                             a->inv_dx, 0, a->mdot_part, s);
         if (a->o.accretion_radius > 0.0)
-            launch_mdot_sum(a->mdot_part, face_kernel_blocks(b, 32),
+            launch_mdot_sum(a->mdot_part, face_kernel_blocks(b, 0),
                             a->dt / 6.0 * stage_weight(st), a->mdot_acc, s);
         k_adj_bits<<<gg, 256, 0, s>>>(b, a->o, sl.P[st], sl.bits[st]);
         double *out = (st < 3) ? sl.U[st + 1] : next;
@@ -620,7 +620,7 @@ int grhd_adjoint_create(const grhd_params *params, const grhd_box *box,
     a->grid = sms * 8;
 
     const size_t gv = (size_t)a->b.gvol(), iv = (size_t)a->b.ivol();
-    const size_t nfb = (size_t)face_kernel_blocks(a->b, 32);
+    const size_t nfb = (size_t)face_kernel_blocks(a->b, 0);
     size_t off = 0;
     std::vector<size_t> offs;
     auto take = [&](size_t bytes) {

@@ -54,7 +54,7 @@ struct grhd_ctx
     DevStatus *status_h = nullptr; // pinned host mirror
     double *probe = nullptr;       // device scalars: probe + torus setup
     int *flag = nullptr;           // device flag (initial-data failures)
-    int zchunk = 32;
+    int zchunk = 0; // face kernel z march: chosen per box (face_zchunk)
     grhd_error last_error;
     // instrumentation
     long long launches = 0;
@@ -276,6 +276,14 @@ int grow(grhd_ctx *ctx, double **ptr, size_t *cap, size_t need)
     return GRHD_OK;
 }
 
+// blocks of one face-kernel launch over box b (its z march as chosen for
+// the context's precision)
+int64_t face_blocks(const grhd_ctx *ctx, const BoxDev &b)
+{
+    return face_kernel_blocks(b, ctx->zchunk,
+                              ctx->params.precision == GRHD_PRECISION_MIXED);
+}
+
 int ensure_scratch(grhd_ctx *ctx, const BoxDev &b, bool need_stage)
 {
     int st = grow(ctx, &ctx->prim, &ctx->prim_cap, 5 * (size_t)b.gvol());
@@ -297,7 +305,7 @@ int ensure_scratch(grhd_ctx *ctx, const BoxDev &b, bool need_stage)
         return st;
     if (ctx->params.accretion_radius > 0.0)
         st = grow(ctx, &ctx->mdot_part, &ctx->mdot_cap,
-                  (size_t)face_kernel_blocks(b, ctx->zchunk));
+                  (size_t)face_blocks(ctx, b));
     return st;
 }
 
@@ -420,7 +428,7 @@ void enqueue_rhs(grhd_ctx *ctx, T *rhs, double *state, const BoxDev &b,
     if (ctx->params.accretion_radius > 0.0)
     {
         ++ctx->launches;
-        launch_mdot_sum(ctx->mdot_part, face_kernel_blocks(b, ctx->zchunk),
+        launch_mdot_sum(ctx->mdot_part, face_blocks(ctx, b),
                         mdot_weight, ctx->mdot_acc, s);
     }
 }
@@ -1094,8 +1102,8 @@ int enqueue_rk4_host_pipelined(grhd_ctx *ctx, double *host, double *dev,
     T *P[2] = {scratch<T>(ctx->prim), scratch<T>(ctx->prim2)};
     T *k = scratch<T>(ctx->kbuf), *src = scratch<T>(ctx->src);
     double *acc = ctx->acc;
-    // a chunk is a few dozen planes: face blocks of 8 planes fill the GPU
-    const int zc = std::min(ctx->zchunk, 8);
+    // the z march of each chunk's face blocks chosen for the chunk
+    const int zc = ctx->zchunk;
     for (int w = 0; w < z.n + 4; ++w)
     {
         if (w < z.n)
@@ -2563,7 +2571,7 @@ void enqueue_rhs_static(grhd_ctx *ctx, T *rhs, double *state, const BoxDev &b,
     if (ctx->params.accretion_radius > 0.0)
     {
         ++ctx->launches;
-        launch_mdot_sum(mdot_part, face_kernel_blocks(b, ctx->zchunk), 0.0,
+        launch_mdot_sum(mdot_part, face_blocks(ctx, b), 0.0,
                         ctx->mdot_acc, s);
     }
 }
@@ -2598,13 +2606,13 @@ extern "C" int grhd_compute_rhs_static(grhd_ctx *ctx, double *rhs,
         return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, nullptr,
                          0.0, msg);
     }
-    if (face_kernel_blocks(b, ctx->zchunk) > kStaticMdotBlocks)
+    if (face_blocks(ctx, b) > kStaticMdotBlocks)
     {
         char msg[200];
         std::snprintf(msg, sizeof(msg),
                       "box too large for the static RHS scratch: its face "
                       "pass needs %lld accretion partials (limit %lld)",
-                      (long long)face_kernel_blocks(b, ctx->zchunk),
+                      (long long)face_blocks(ctx, b),
                       (long long)kStaticMdotBlocks);
         return set_error(ctx, GRHD_ERR_INVALID_ARG, GRHD_WHERE_NONE, nullptr,
                          0.0, msg);

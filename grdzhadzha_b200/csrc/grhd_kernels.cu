@@ -24,6 +24,8 @@
 // here the interface states never leave registers / shared memory.
 #include "grhd_kernels.cuh"
 
+#include <atomic>
+
 namespace grhd {
 
 namespace {
@@ -2166,10 +2168,99 @@ template cudaError_t launch_ensemble<double>(const EnsLaunch &, int,
 template cudaError_t launch_ensemble<float>(const EnsLaunch &, int,
                                             cudaStream_t);
 
-int64_t face_kernel_blocks(const BoxDev &b, int zchunk)
+namespace
 {
-    if (zchunk < 1)
-        zchunk = 1;
+// resident face-kernel blocks of the current device (SMs x blocks per SM
+// at the kernel's registers and shared memory), per precision
+int face_slots(bool fp32)
+{
+    static std::atomic<int> cache[64][2];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+        return fp32 ? 3 * 148 : 2 * 148;
+    std::atomic<int> &c = cache[dev][fp32 ? 1 : 0];
+    const int have = c.load(std::memory_order_relaxed);
+    if (have > 0)
+        return have;
+    int sms = 148, per = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const cudaError_t e =
+        fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                   &per, k_faces<float, false, 0>, kTB * kTB,
+                   faces_smem<float>())
+             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                   &per, k_faces<double, false, 0>, kTB * kTB,
+                   faces_smem<double>());
+    if (e != cudaSuccess || per < 1)
+    {
+        (void)cudaGetLastError();
+        per = fp32 ? 3 : 2;
+    }
+    c.store(sms * per, std::memory_order_relaxed);
+    return sms * per;
+}
+} // namespace
+
+// Makespan (in plane-times) of nf blocks of df planes followed by np of dp
+// planes on `slots` resident blocks, each block started on the slot that
+// frees first in launch order (the last z row of a launch holds the short
+// blocks): whole waves of full blocks, then the short blocks on the slots
+// left free in the last full wave and on the others as they free.
+int64_t face_makespan(int64_t nf, int64_t df, int64_t np, int64_t dp,
+                      int64_t slots)
+{
+    const int64_t t1 = (nf / slots) * df, rem = nf % slots;
+    int64_t ta = t1, na = slots - rem;           // free at t1
+    int64_t tb = t1 + (rem ? df : 0), nb = rem;  // free after the last full
+    int64_t end = rem ? tb : t1;
+    for (int64_t left = np; left > 0;)
+    {
+        if (nb == 0 || ta <= tb)
+        {
+            left -= std::min(left, na);
+            ta += dp;
+            end = std::max(end, ta);
+        }
+        else
+        {
+            left -= std::min(left, nb);
+            tb += dp;
+            end = std::max(end, tb);
+        }
+    }
+    return end;
+}
+
+int face_zchunk(const BoxDev &b, int zchunk, bool fp32)
+{
+    if (zchunk > 0)
+        return zchunk;
+    const int64_t slots = face_slots(fp32);
+    const int64_t tiles =
+        (int64_t)((b.in[0] + kTC - 1) / kTC) * ((b.in[1] + kTC - 1) / kTC);
+    const int nz = b.in[2];
+    const int cand[5] = {32, 16, 8, 6, 4};
+    int best = cand[0];
+    int64_t best_cost = -1;
+    for (int z : cand)
+    {
+        // nz / z full blocks per column of tiles, then one of nz % z
+        // planes; every block also marches two lead-in planes
+        const int r = nz % z;
+        const int64_t cost = face_makespan(tiles * (nz / z), z + 2,
+                                           r ? tiles : 0, r + 2, slots);
+        if (best_cost < 0 || cost < best_cost)
+        {
+            best = z;
+            best_cost = cost;
+        }
+    }
+    return best;
+}
+
+int64_t face_kernel_blocks(const BoxDev &b, int zchunk, bool fp32)
+{
+    zchunk = face_zchunk(b, zchunk, fp32);
     return (int64_t)((b.in[0] + kTC - 1) / kTC) * ((b.in[1] + kTC - 1) / kTC) *
            ((b.in[2] + zchunk - 1) / zchunk);
 }
@@ -2213,8 +2304,7 @@ void launch_faces(const T *prim, const T *src, T *rhs, const BoxDev &b,
                   const double inv_dx[3], int zchunk, double *mdot_part,
                   cudaStream_t s)
 {
-    if (zchunk < 1)
-        zchunk = 1;
+    zchunk = face_zchunk(b, zchunk, sizeof(T) == sizeof(float));
     dim3 grid((b.in[0] + kTC - 1) / kTC, (b.in[1] + kTC - 1) / kTC,
               (b.in[2] + zchunk - 1) / zchunk);
     dim3 block(kTB, kTB);

@@ -137,7 +137,13 @@ constexpr int kGeoFields = 16;
 
 // Per-device kernel attributes (dynamic shared memory of the face kernels).
 cudaError_t configure_kernels();
-int64_t face_kernel_blocks(const BoxDev &b, int zchunk);
+// z-march length (planes per block) of the face kernel for box b: zchunk
+// when positive; otherwise the one of 32, 16, 8, 6, 4 planes with the
+// shortest makespan ceil(blocks / resident blocks of the device) x
+// (planes + 2) (a block marches its planes after two lead-in planes; the
+// RHS does not depend on the choice).
+int face_zchunk(const BoxDev &b, int zchunk, bool fp32);
+int64_t face_kernel_blocks(const BoxDev &b, int zchunk, bool fp32 = false);
 
 // T is the arithmetic type of the primitive cache, sources and RHS:
 // double (FP64 path) or float (mixed path).
