@@ -617,7 +617,9 @@ int grhd_adjoint_create(const grhd_params *params, const grhd_box *box,
         a->inv_dx[d] = 1.0 / params->dx;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, a->device);
-    a->grid = sms * 8;
+    // a whole number of waves for the reverse cell kernel (2 blocks of 128
+    // threads per SM) and the reverse face kernels (3 per SM)
+    a->grid = sms * 6;
 
     const size_t gv = (size_t)a->b.gvol(), iv = (size_t)a->b.ivol();
     const size_t nfb = (size_t)face_kernel_blocks(a->b, 0);

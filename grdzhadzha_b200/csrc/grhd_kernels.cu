@@ -529,6 +529,55 @@ __device__ __forceinline__ PVT<T> load_pv_smem(const T *P, int cell)
     return p;
 }
 
+// Asynchronous global -> shared copy of one element (cp.async, 4 or 8
+// bytes, cached in L1) and the wait for all of this thread's copies.
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d),
+                     "l"(src)
+                     : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d),
+                     "l"(src)
+                     : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// The primitive cross tile of a z march at plane k (clamped to the
+// ghosted box): synchronous loads, or (ASYNC) cp.async copies completed by
+// cp_async_wait_all before the next barrier.
+template <typename T, bool CG, bool ASYNC>
+__device__ __forceinline__ void load_p_tile(T *P, const T *__restrict__ prim,
+                                            const BoxDev &b, int i0, int j0,
+                                            int k, int tid)
+{
+    constexpr int nP = kPW * kPW;
+    for (int idx = tid; idx < nP; idx += kTB * kTB)
+    {
+        const int u = idx % kPW, v = idx / kPW;
+        if ((u < 2 || u > kPW - 3) && (v < 2 || v > kPW - 3))
+            continue;
+        const int gi = min(max(i0 - 2 + u, b.glo[0]), b.ghi[0]);
+        const int gj = min(max(j0 - 2 + v, b.glo[1]), b.ghi[1]);
+        const int64_t g = b.gidx(gi, gj, k);
+#pragma unroll
+        for (int c = 0; c < 5; ++c)
+        {
+            if constexpr (ASYNC)
+                cp_async_elem(&P[c * nP + idx], &prim[c * b.pcs + g]);
+            else
+                P[c * nP + idx] = rdro<CG>(&prim[c * b.pcs + g]);
+        }
+    }
+}
+
 // Geometry of the cross-shaped (x,y) neighbourhood of a tile at plane kk.
 template <typename T, int BGK = -1>
 __device__ __forceinline__ void tile_geometry(T *G, const Background &bg,
@@ -654,21 +703,15 @@ faces_tile(const T *__restrict__ prim, const T *__restrict__ src,
         const bool cells = k >= k0;     // plane k's x/y faces and RHS
         if (zface)
             w3 = load_pv_global<T, CG>(prim, b.pcs, b.gidx(ci_c, cj_c, k + 2));
-        // primitive cross tile at plane k (clamped to the ghosted box)
-        if (cells)
-            for (int idx = tid; idx < nP; idx += kTB * kTB)
-            {
-                const int u = idx % kPW, v = idx / kPW;
-                if ((u < 2 || u > kPW - 3) && (v < 2 || v > kPW - 3))
-                    continue;
-                const int gi = min(max(i0 - 2 + u, b.glo[0]), b.ghi[0]);
-                const int gj = min(max(j0 - 2 + v, b.glo[1]), b.ghi[1]);
-                const int64_t g = b.gidx(gi, gj, k);
-#pragma unroll
-                for (int c = 0; c < 5; ++c)
-                    P[c * nP + idx] = rdro<CG>(&prim[c * b.pcs + g]);
-            }
+        // primitive cross tile at plane k: issued after the previous
+        // plane's faces (asynchronous copies, overlapping that plane's
+        // output and this plane's geometry), or loaded here (the ensemble's
+        // coherent loads)
+        if (cells && CG)
+            load_p_tile<T, CG, false>(P, prim, b, i0, j0, k, tid);
         tile_geometry<T, BGK>(Gn, bg, o, i0, j0, k + 1, tid);
+        if (cells && !CG)
+            cp_async_wait_all();
         __syncthreads();
 
         // x face between cells (i0+a-1, i0+a) in row j0+bb
@@ -726,6 +769,9 @@ faces_tile(const T *__restrict__ prim, const T *__restrict__ src,
                 macc += mdot_face(o, ci, cj, k, 2, gf, Fhi.D);
         }
         __syncthreads();
+        // the x/y faces have read plane k's tile: fetch plane k+1's
+        if (!CG && k + 1 >= k0 && k + 1 <= k1)
+            load_p_tile<T, CG, true>(P, prim, b, i0, j0, k + 1, tid);
 
         if (cells && col_ok)
         {
