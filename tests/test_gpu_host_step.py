@@ -81,3 +81,35 @@ def test_host_step_rejects_a_box_that_is_not_the_domain():
     host = lv.state.cpu()
     with pytest.raises(G.InvalidArgument):
         op.advance_rk4_cfl_host(host, lv, 0.25)
+
+
+@pytest.mark.parametrize("cell,where", [((13, 14, 17), 2), ((0, 9, 17), 1)])
+def test_host_step_recovery_failure_matches_the_device_step(cell, where):
+    """A planted D < 0 (host-side; no device fault) in the third of four
+    z chunks: the wavefront host step (given the CFL speed) fails with the
+    device step's error record (the cell's recovery, or for a boundary cell
+    the outflow fill of its ghosts first), returns only after its copies
+    have finished, and the context steps cleanly afterwards."""
+    import grdzhadzha_b200 as G
+    p, box, s, t = cases.CASES["torus_a09"]()
+    i, j, k = cell
+    g = [box.lo[d] - box.glo[d] for d in range(3)]
+    bad = s.copy()
+    O.state_view(box, bad)[O.D, g[2] + k, g[1] + j, g[0] + i] = -1.0
+    op = cases.gpu_operator(p)
+    lv = cases.gpu_level(box, bad)
+    host = torch.from_numpy(bad.copy()).reshape(lv.state.shape).pin_memory()
+    mi = op.compute_max_inverse_dt(cases.gpu_level(box, s), time=t)
+    with pytest.raises(G.GRHDError) as eh:
+        op.advance_rk4_cfl_host(host, lv, 0.25, time=t, max_inverse_dt=mi)
+    with pytest.raises(G.GRHDError) as ed:
+        op.advance_rk4_cfl(lv, 0.25, time=t, max_inverse_dt=mi)
+    assert (eh.value.where, eh.value.cell) == (ed.value.where, ed.value.cell)
+    assert eh.value.where == where and eh.value.cell == cell
+    good = torch.from_numpy(s.copy()).reshape(lv.state.shape).pin_memory()
+    dev = cases.gpu_level(box, s)
+    dt_h, mi_h, _, _, _ = op.advance_rk4_cfl_host(good, dev, 0.25, time=t,
+                                                  max_inverse_dt=mi)
+    dt_d, mi_d, _ = op.advance_rk4_cfl(dev, 0.25, time=t, max_inverse_dt=mi)
+    assert (dt_h, mi_h) == (dt_d, mi_d)
+    assert torch.equal(good, dev.state.cpu())
