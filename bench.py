@@ -637,7 +637,7 @@ def run_widened(hbm_peak):
         "value": cells / (ms / 1e3), "unit": "cell-RHS/s", "ms": ms,
         "fixed_background_rhs_ms": ms_f,
         "hbm_frac": alg / (ms / 1e3) / 1e9 / hbm_peak,
-        "note": "FP64, every face twice, not tiled yet"}
+        "note": "FP64, one thread per cell, each face evaluated by both of its cells (a face-tiled version measured slower)"}
     del lv36, rhs, cop
     # multi-box level: 256^3 cut into 8 z-slabs, exchange + split SSPRK2
     n = 256

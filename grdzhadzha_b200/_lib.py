@@ -205,6 +205,7 @@ SIGNATURES = {
                                        _vp]),
     "grhd_eval_con2prim": (C.c_int, [_vp, C.c_int64, _vp, _vp, _vp, _vp, _vp,
                                      _vp, _vp]),
+    "grhd_eval_arith": (C.c_int, [_vp, C.c_int64, _vp, _vp, _vp, _vp]),
     "grhd_default_torus_config": (None, [_P(TorusConfig)]),
     "grhd_torus_initial_data": (C.c_int, [_vp, _vp, C.c_int64, _P(Box),
                                           _P(TorusConfig), C.c_double,

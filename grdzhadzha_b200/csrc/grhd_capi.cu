@@ -1701,6 +1701,18 @@ int grhd_eval_con2prim(grhd_ctx *ctx, int64_t n, const double *cons,
     return GRHD_OK;
 }
 
+int grhd_eval_arith(grhd_ctx *ctx, int64_t n, const double *a,
+                    const double *b, double *out, void *stream)
+{
+    if (!ctx || n < 0 || (n > 0 && (!a || !b || !out)))
+        return GRHD_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    launch_eval_arith(n, a, b, out, s);
+    GRHD_CUDA(ctx, cudaGetLastError());
+    GRHD_CUDA(ctx, cudaStreamSynchronize(s));
+    return GRHD_OK;
+}
+
 void grhd_default_torus_config(grhd_torus_config *c)
 {
     // FixedBGTorusConfig defaults, FixedBGTorus.hpp:20-34

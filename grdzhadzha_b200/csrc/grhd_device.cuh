@@ -28,16 +28,61 @@ __host__ __device__ constexpr int sym(int i, int j)
 }
 
 // ------------------------------------------------------------- arithmetic
-// FP64: IEEE division and square root exactly as written in the
-// reference's expressions.  FP32: the SFU reciprocal / reciprocal square
-// root (a few ulp), which is what makes the FP32 path cheap.
+// FP64 on the device: division, reciprocal and square root from the
+// hardware's approximate reciprocal (square root) refined by Newton-Raphson
+// steps, within about one ulp of the IEEE result (checked against it by
+// grhd_eval_arith's test) and without the IEEE operations' special-case
+// branches, which the face and stage kernels pay on every call.  Their
+// domain is that of the quantities they are used on -- densities,
+// enthalpies, metric functions, speed differences and squared norms:
+// normal numbers up to 2^1021, and 0 for the square root; a zero divisor
+// or a quotient that overflows gives NaN (not +-inf), and a subnormal
+// operand is flushed to zero.  The oracle, the host and the FP64 con2prim
+// (written with the operators) keep IEEE division.  FP32: the SFU
+// reciprocal / reciprocal square root (a few ulp), which is what makes the
+// FP32 path cheap.
 
-GRHD_HD __forceinline__ double div_(double a, double b) { return a / b; }
+#ifdef __CUDA_ARCH__
+// 1/a: the approximate reciprocal (rcp.approx.ftz.f64, about 20 correct
+// bits) and two Newton-Raphson steps y <- y + y (1 - a y), each of which
+// squares the relative error.
+__device__ __forceinline__ double rcp_newton(double a)
+{
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(a));
+#pragma unroll
+    for (int it = 0; it < 2; ++it)
+        y = fma(y, fma(-a, y, 1.0), y);
+    return y;
+}
+#endif
+
+// a / b: the quotient q = a y with y ~ 1/b, corrected once by its exact
+// residual r = a - b q (one fused multiply-add): q + r y (Markstein's
+// correction, IBM J. Res. Dev. 34 (1990) 111-119).
+GRHD_HD __forceinline__ double div_(double a, double b)
+{
+#ifdef __CUDA_ARCH__
+    const double y = rcp_newton(b);
+    const double q = a * y;
+    return fma(fma(-b, q, a), y, q);
+#else
+    return a / b;
+#endif
+}
 __device__ __forceinline__ float div_(float a, float b)
 {
     return __fdividef(a, b);
 }
-GRHD_HD __forceinline__ double rcp_(double a) { return 1.0 / a; }
+GRHD_HD __forceinline__ double rcp_(double a)
+{
+#ifdef __CUDA_ARCH__
+    const double y = rcp_newton(a);
+    return fma(y, fma(-a, y, 1.0), y);
+#else
+    return 1.0 / a;
+#endif
+}
 __device__ __forceinline__ float rcp_(float a) { return __fdividef(1.0f, a); }
 // FP64 reciprocal square root: the hardware's approximate rsqrt
 // (rsqrt.approx.ftz.f64, a few ulp of FP32 accuracy) refined by two
@@ -63,7 +108,21 @@ GRHD_HD __forceinline__ double rsqrt_(double a)
 #endif
 }
 __device__ __forceinline__ float rsqrt_(float a) { return rsqrtf(a); }
-GRHD_HD __forceinline__ double sqrt_(double a) { return sqrt(a); }
+// sqrt(a) = a / sqrt(a): s = a y with y ~ 1/sqrt(a) (rsqrt_), corrected by
+// one Newton step on s^2 = a, s + (a - s^2) y / 2; a = 0 returns 0 and a
+// negative a NaN.
+GRHD_HD __forceinline__ double sqrt_(double a)
+{
+#ifdef __CUDA_ARCH__
+    const double y = rsqrt_(a);
+    const double s = a * y;
+    const double r = fma(0.5 * y, fma(-s, s, a), s);
+    return a > 0.0 ? r
+                   : (a == 0.0 ? a : __longlong_as_double(0x7ff8000000000000ll));
+#else
+    return sqrt(a);
+#endif
+}
 __device__ __forceinline__ float sqrt_(float a) { return sqrtf(a); }
 GRHD_HD __forceinline__ double max_(double a, double b) { return fmax(a, b); }
 __device__ __forceinline__ float max_(float a, float b) { return fmaxf(a, b); }

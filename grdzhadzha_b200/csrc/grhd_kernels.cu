@@ -1410,6 +1410,20 @@ __global__ void k_eval_con2prim(int64_t n, const double *__restrict__ cons,
         prim[6 * t + 3 + i] = pr.v[i];
 }
 
+// The FP64 division, reciprocal and square root of the kernels at n
+// points: out[3t .. 3t+2] = a/b, 1/b, sqrt(a).
+__global__ void k_eval_arith(int64_t n, const double *__restrict__ a,
+                             const double *__restrict__ b,
+                             double *__restrict__ out)
+{
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n)
+        return;
+    out[3 * t] = div_(a[t], b[t]);
+    out[3 * t + 1] = rcp_(b[t]);
+    out[3 * t + 2] = sqrt_(a[t]);
+}
+
 // ------------------------------------------------------------- ensemble
 
 __device__ __forceinline__ unsigned long long global_ns()
@@ -2459,6 +2473,14 @@ void launch_eval_con2prim(int64_t n, const double *cons, const double *gUU,
     k_eval_con2prim<<<(int)((n + 127) / 128), 128, 0, s>>>(n, cons, gUU, o,
                                                            prim, ok, iters,
                                                            resid);
+}
+
+void launch_eval_arith(int64_t n, const double *a, const double *b,
+                       double *out, cudaStream_t s)
+{
+    if (n <= 0)
+        return;
+    k_eval_arith<<<(int)((n + 255) / 256), 256, 0, s>>>(n, a, b, out);
 }
 
 void launch_ccz4_fill(double *s, const BoxDev &b, bool conserved,

@@ -213,6 +213,8 @@ void launch_eval_background(int64_t n, const double *xyz,
 void launch_eval_con2prim(int64_t n, const double *cons, const double *gUU,
                           const Options &o, double *prim, int *ok, int *iters,
                           double *resid, cudaStream_t s);
+void launch_eval_arith(int64_t n, const double *a, const double *b,
+                       double *out, cudaStream_t s);
 
 // ------------------------------------------------------------ ensemble
 // Many independent boxes (members) advanced by one persistent launch: each
