@@ -37,8 +37,9 @@ __host__ __device__ constexpr int sym(int i, int j)
 // enthalpies, metric functions, speed differences and squared norms:
 // normal numbers up to 2^1021, and 0 for the square root; a zero divisor
 // or a quotient that overflows gives NaN (not +-inf), and a subnormal
-// operand is flushed to zero.  The oracle, the host and the FP64 con2prim
-// (written with the operators) keep IEEE division.  FP32: the SFU
+// operand is flushed to zero.  The oracle and the host keep IEEE
+// division, as does the binary's volume-time source (pn_scalar), whose
+// time difference is rounded as the reference's.  FP32: the SFU
 // reciprocal / reciprocal square root (a few ulp), which is what makes the
 // FP32 path cheap.
 
@@ -626,14 +627,17 @@ GRHD_HD __forceinline__ ConsT<T> p2c(const PrimT<T> &pr, const T gLL[6])
     return c;
 }
 
-// detail::pressure_residual (+ derivative), Valencia.hpp:79-108.
+// detail::pressure_residual (+ derivative), Valencia.hpp:79-108.  The
+// recovery divides with div_ / rcp_ / sqrt_ like the rest of the device
+// code; e = tau + D + p equal to zero (which IEEE division would turn into
+// a capped v^2) gives a NaN residual and so a failed recovery.
 GRHD_HD __forceinline__ double c2p_residual(double p, double D,
                                                double tau, double S2,
                                                double G, double Gfac,
                                                double vmax2, double *deriv)
 {
     const double e = tau + D + p;
-    const double ie = 1.0 / e;
+    const double ie = rcp_(e);
     double v2 = S2 * ie * ie;
     if (v2 > vmax2)
         v2 = vmax2;
@@ -662,14 +666,18 @@ GRHD_HD __forceinline__ bool c2p_finish(const Options &o, const Cons &c,
                                            double p, Prim &out)
 {
     const double e = c.tau + c.D + p;
-    const double v2 = S2 / (e * e);
+    const double v2 = div_(S2, e * e);
     if (!(v2 < o.rec_vmax2))
         return false;
-    const double W = 1.0 / sqrt(1.0 - v2);
-    out.rho = c.D / W;
+    // W rounded as the reference's 1 / sqrt(1 - v^2) (sqrt_ and rcp_ give
+    // the IEEE results, rsqrt_ is up to two ulp off): rho = D / W decides
+    // the atmosphere and floor tests bit for bit, and an ulp there switches
+    // a cell's sources on or off
+    const double W = rcp_(sqrt_(1.0 - v2));
+    out.rho = div_(c.D, W);
     out.p = p;
-    out.eps = p / ((o.G - 1.0) * out.rho);
-    const double ie = 1.0 / e;
+    out.eps = div_(p, (o.G - 1.0) * out.rho);
+    const double ie = rcp_(e);
     out.v[0] = (gUU[0] * c.S[0] + gUU[1] * c.S[1] + gUU[2] * c.S[2]) * ie;
     out.v[1] = (gUU[1] * c.S[0] + gUU[3] * c.S[1] + gUU[4] * c.S[2]) * ie;
     out.v[2] = (gUU[2] * c.S[0] + gUU[4] * c.S[1] + gUU[5] * c.S[2]) * ie;
@@ -687,7 +695,7 @@ GRHD_HD __forceinline__ bool con2prim(const Options &o, const Cons &c,
     if (c.D > 0.0)
     {
         const double G = o.G;
-        const double Gfac = G / (G - 1.0);
+        const double Gfac = div_(G, G - 1.0);
         const double vmax2 = o.rec_vmax2;
         const double tol = o.rec_tol;
         const double S2 = c2p_S2(c, gUU);
@@ -728,7 +736,7 @@ GRHD_HD __forceinline__ bool con2prim(const Options &o, const Cons &c,
                     else
                         lower = p;
                 }
-                double np = p - r / dres;
+                double np = p - div_(r, dres);
                 if (!isfinite(np) || np <= lower || np >= upper)
                     np = 0.5 * (lower + upper);
                 p = np;
@@ -763,7 +771,7 @@ GRHD_HD __forceinline__ bool con2prim_warm(const Options &o, const Cons &c,
         const double G = o.G;
         const double S2 = c2p_S2(c, gUU);
         const double r = c2p_residual(o.rec_pfloor, c.D, c.tau, S2, G,
-                                      G / (G - 1.0), o.rec_vmax2, nullptr);
+                                      div_(G, G - 1.0), o.rec_vmax2, nullptr);
         if (fabs(r) <= o.rec_tol)
             return c2p_finish(o, c, gUU, S2, o.rec_pfloor, out) ||
                    con2prim(o, c, gUU, out, nullptr, nullptr);
@@ -771,7 +779,7 @@ GRHD_HD __forceinline__ bool con2prim_warm(const Options &o, const Cons &c,
     if (c.D > 0.0 && p_guess > o.rec_pfloor && isfinite(p_guess))
     {
         const double G = o.G;
-        const double Gfac = G / (G - 1.0);
+        const double Gfac = div_(G, G - 1.0);
         const double S2 = c2p_S2(c, gUU);
         double p = p_guess, dres;
         double r = c2p_residual(p, c.D, c.tau, S2, G, Gfac, o.rec_vmax2, &dres);
@@ -780,7 +788,7 @@ GRHD_HD __forceinline__ bool con2prim_warm(const Options &o, const Cons &c,
             if (fabs(r) < o.rec_tol)
                 return c2p_finish(o, c, gUU, S2, p, out) ||
                        con2prim(o, c, gUU, out, nullptr, nullptr);
-            const double np = p - r / dres;
+            const double np = p - div_(r, dres);
             if (!isfinite(np) || !(np > o.rec_pfloor))
                 break;
             p = np;

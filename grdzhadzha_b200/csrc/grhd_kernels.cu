@@ -1410,8 +1410,9 @@ __global__ void k_eval_con2prim(int64_t n, const double *__restrict__ cons,
         prim[6 * t + 3 + i] = pr.v[i];
 }
 
-// The FP64 division, reciprocal and square root of the kernels at n
-// points: out[3t .. 3t+2] = a/b, 1/b, sqrt(a).
+// The FP64 division, reciprocal, square root and reciprocal square root
+// of the kernels at n points: out[4t .. 4t+3] = a/b, 1/b, sqrt(a),
+// 1/sqrt(a).
 __global__ void k_eval_arith(int64_t n, const double *__restrict__ a,
                              const double *__restrict__ b,
                              double *__restrict__ out)
@@ -1419,9 +1420,10 @@ __global__ void k_eval_arith(int64_t n, const double *__restrict__ a,
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t >= n)
         return;
-    out[3 * t] = div_(a[t], b[t]);
-    out[3 * t + 1] = rcp_(b[t]);
-    out[3 * t + 2] = sqrt_(a[t]);
+    out[4 * t] = div_(a[t], b[t]);
+    out[4 * t + 1] = rcp_(b[t]);
+    out[4 * t + 2] = sqrt_(a[t]);
+    out[4 * t + 3] = rsqrt_(a[t]);
 }
 
 // ------------------------------------------------------------- ensemble

@@ -329,10 +329,11 @@ int grhd_eval_con2prim(grhd_ctx *ctx, int64_t n, const double *cons,
                        const double *gUU, double *prim, int *ok,
                        int *iterations, double *residual, void *stream);
 
-/* The FP64 division, reciprocal and square root the kernels compute with,
- * at n points: out[3n] = (a/b, 1/b, sqrt(a)) per point (about one ulp from
- * IEEE for normal operands and results, and 0 for the square root; a zero
- * divisor or an overflowing quotient gives NaN).  New (the reference
+/* The FP64 division, reciprocal, square root and reciprocal square root
+ * the kernels compute with, at n points: out[4n] = (a/b, 1/b, sqrt(a),
+ * 1/sqrt(a)) per point (about one ulp from IEEE for normal operands and
+ * results, and 0 for the square root; a zero divisor or an overflowing
+ * quotient gives NaN).  New (the reference
  * uses IEEE operations).  Device pointers. */
 int grhd_eval_arith(grhd_ctx *ctx, int64_t n, const double *a,
                     const double *b, double *out, void *stream);
