@@ -493,40 +493,41 @@ GRHD_HD inline void con2prim_rev(const Options &o, const Cons &c,
 {
     const double S2 = c2p_S2(c, gUU);
     const double e = c.tau + c.D + p;
-    const double v2 = S2 / (e * e);
-    const double W = 1.0 / sqrt(1.0 - v2);
-    const double rho = c.D / W;
+    const double v2 = div_(S2, e * e);
+    const double W = rcp_(sqrt_(1.0 - v2));
+    const double rho = div_(c.D, W);
     const double gm1 = o.G - 1.0;
-    const double eps = p / (gm1 * rho);
+    const double eps = div_(p, gm1 * rho);
     double m[3];
     lower(gUU, c.S, m);
-    double pbar = pb.p + pb.eps / (gm1 * rho);
-    const double rhobar = pb.rho - pb.eps * eps / rho;
-    cb.D += rhobar / W;
-    const double Wbar = -rhobar * rho / W;
+    double pbar = pb.p + div_(pb.eps, gm1 * rho);
+    const double rhobar = pb.rho - div_(pb.eps * eps, rho);
+    cb.D += div_(rhobar, W);
+    const double Wbar = div_(-rhobar * rho, W);
+    const double ie = rcp_(e);
     double mbar[3], ebar = 0.0;
     for (int i = 0; i < 3; ++i)
     {
-        mbar[i] = pb.v[i] / e;
-        ebar -= pb.v[i] * m[i] / (e * e);
+        mbar[i] = pb.v[i] * ie;
+        ebar -= pb.v[i] * m[i] * ie * ie;
     }
     const double v2bar = Wbar * 0.5 * W * W * W;
-    double S2bar = v2bar / (e * e);
-    ebar -= 2.0 * v2bar * v2 / e;
+    double S2bar = v2bar * ie * ie;
+    ebar -= 2.0 * v2bar * v2 * ie;
     cb.tau += ebar;
     cb.D += ebar;
     pbar += ebar;
     if (p > o.rec_pfloor)
     {
-        const double Gfac = o.G / gm1;
+        const double Gfac = div_(o.G, gm1);
         const double fW = c.D + 2.0 * Gfac * p * W;
         const double dWdv2 = 0.5 * W * W * W;
-        const double dv2de = -2.0 * v2 / e;
+        const double dv2de = -2.0 * v2 * ie;
         const double f_p = Gfac * W * W + fW * dWdv2 * dv2de - 1.0;
         const double f_D = W + fW * dWdv2 * dv2de - 1.0;
         const double f_tau = fW * dWdv2 * dv2de - 1.0;
-        const double f_S2 = fW * dWdv2 / (e * e);
-        const double q = -pbar / f_p;
+        const double f_S2 = fW * dWdv2 * ie * ie;
+        const double q = div_(-pbar, f_p);
         cb.D += q * f_D;
         cb.tau += q * f_tau;
         S2bar += q * f_S2;
@@ -550,12 +551,12 @@ GRHD_HD inline Prim c2p_at(const Options &o, const Cons &c,
     Prim out;
     const double S2 = c2p_S2(c, gUU);
     const double e = c.tau + c.D + p;
-    const double v2 = S2 / (e * e);
-    const double W = 1.0 / sqrt(1.0 - v2);
-    out.rho = c.D / W;
+    const double v2 = div_(S2, e * e);
+    const double W = rcp_(sqrt_(1.0 - v2));
+    out.rho = div_(c.D, W);
     out.p = p;
-    out.eps = p / ((o.G - 1.0) * out.rho);
-    const double ie = 1.0 / e;
+    out.eps = div_(p, (o.G - 1.0) * out.rho);
+    const double ie = rcp_(e);
     out.v[0] = (gUU[0] * c.S[0] + gUU[1] * c.S[1] + gUU[2] * c.S[2]) * ie;
     out.v[1] = (gUU[1] * c.S[0] + gUU[3] * c.S[1] + gUU[4] * c.S[2]) * ie;
     out.v[2] = (gUU[2] * c.S[0] + gUU[4] * c.S[1] + gUU[5] * c.S[2]) * ie;
@@ -575,8 +576,8 @@ GRHD_HD inline void static_sources_rev(const Prim &pr, const Cons &c,
     double vL[3];
     lower(g.gLL, pr.v, vL);
     const double v2 = vL[0] * pr.v[0] + vL[1] * pr.v[1] + vL[2] * pr.v[2];
-    const double W = 1.0 / sqrt(1.0 - v2);
-    const double h = 1.0 + pr.eps + pr.p / pr.rho;
+    const double W = rsqrt_(1.0 - v2);
+    const double h = 1.0 + pr.eps + div_(pr.p, pr.rho);
     const double rhw = pr.rho * h * W * W;
     double st[6];
     for (int i = 0; i < 3; ++i)
@@ -668,8 +669,8 @@ GRHD_HD inline void static_sources_rev(const Prim &pr, const Cons &c,
     const double hbar = rhwbar * pr.rho * W * W;
     const double Wbar = rhwbar * pr.rho * h * 2.0 * W;
     pb.eps += hbar;
-    pb.p += hbar / pr.rho;
-    pb.rho -= hbar * pr.p / (pr.rho * pr.rho);
+    pb.p += div_(hbar, pr.rho);
+    pb.rho -= div_(hbar * pr.p, pr.rho * pr.rho);
     vsq_rev(pr.v, g.gLL, Wbar * 0.5 * W * W * W, pb.v, fb.g.gLL);
     for (int d = 0; d < 3; ++d)
         phys_flux_rev(pr, c, d, g.lapse, g.shift, Fb[d], pb, cb, fb.g.lapse,

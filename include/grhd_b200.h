@@ -182,7 +182,8 @@ int grhd_compute_rhs(grhd_ctx *ctx, double *rhs, int64_t rhs_comp_stride,
  * leaves the cached address stale.  All calls on a device share the
  * array, so calls that overlap in time there (other streams, threads or
  * contexts) race: issue them one after another.  Like grhd_compute_rhs,
- * the call synchronizes `stream` to read the status word.  Its kernels
+ * the call synchronizes `stream` to read the status word, so it cannot be
+ * captured in a CUDA graph.  Its kernels
  * count in the context's launch counter but not in the per-kernel
  * profile (grhd_profile_read). */
 int grhd_compute_rhs_static(grhd_ctx *ctx, double *rhs,
