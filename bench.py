@@ -638,6 +638,10 @@ def run_widened(hbm_peak):
         "fixed_background_rhs_ms": ms_f,
         "hbm_frac": alg / (ms / 1e3) / 1e9 / hbm_peak,
         "note": "FP64, one thread per cell, each face evaluated by both of its cells (a face-tiled version measured slower)"}
+    out["fixed_background_rhs_128"] = {
+        "value": cells / (ms_f / 1e3), "unit": "cell-RHS/s", "ms": ms_f,
+        "note": "one FP64 compute_rhs of the fixed-background operator "
+                "(ghost fill, per-cell pass, face pass) on the same grid"}
     del lv36, rhs, cop
     # multi-box level: 256^3 cut into 8 z-slabs, exchange + split SSPRK2
     n = 256
