@@ -206,6 +206,8 @@ SIGNATURES = {
     "grhd_eval_con2prim": (C.c_int, [_vp, C.c_int64, _vp, _vp, _vp, _vp, _vp,
                                      _vp, _vp]),
     "grhd_eval_arith": (C.c_int, [_vp, C.c_int64, _vp, _vp, _vp, _vp]),
+    "grhd_face_zchunk": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int,
+                                   C.POINTER(C.c_int)]),
     "grhd_default_torus_config": (None, [_P(TorusConfig)]),
     "grhd_torus_initial_data": (C.c_int, [_vp, _vp, C.c_int64, _P(Box),
                                           _P(TorusConfig), C.c_double,

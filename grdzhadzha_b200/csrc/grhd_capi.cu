@@ -1701,6 +1701,15 @@ int grhd_eval_con2prim(grhd_ctx *ctx, int64_t n, const double *cons,
     return GRHD_OK;
 }
 
+int grhd_face_zchunk(int nx, int ny, int nz, int resident_blocks,
+                     int *zchunk)
+{
+    if (nx < 1 || ny < 1 || nz < 1 || resident_blocks < 1 || !zchunk)
+        return GRHD_ERR_INVALID_ARG;
+    *zchunk = face_zchunk_model(nx, ny, nz, resident_blocks);
+    return GRHD_OK;
+}
+
 int grhd_eval_arith(grhd_ctx *ctx, int64_t n, const double *a,
                     const double *b, double *out, void *stream)
 {

@@ -2297,10 +2297,13 @@ int face_zchunk(const BoxDev &b, int zchunk, bool fp32)
 {
     if (zchunk > 0)
         return zchunk;
-    const int64_t slots = face_slots(fp32);
+    return face_zchunk_model(b.in[0], b.in[1], b.in[2], face_slots(fp32));
+}
+
+int face_zchunk_model(int nx, int ny, int nz, int64_t slots)
+{
     const int64_t tiles =
-        (int64_t)((b.in[0] + kTC - 1) / kTC) * ((b.in[1] + kTC - 1) / kTC);
-    const int nz = b.in[2];
+        (int64_t)((nx + kTC - 1) / kTC) * ((ny + kTC - 1) / kTC);
     const int cand[5] = {32, 16, 8, 6, 4};
     int best = cand[0];
     int64_t best_cost = -1;

@@ -138,11 +138,16 @@ constexpr int kGeoFields = 16;
 // Per-device kernel attributes (dynamic shared memory of the face kernels).
 cudaError_t configure_kernels();
 // z-march length (planes per block) of the face kernel for box b: zchunk
-// when positive; otherwise the one of 32, 16, 8, 6, 4 planes with the
-// shortest makespan ceil(blocks / resident blocks of the device) x
-// (planes + 2) (a block marches its planes after two lead-in planes; the
-// RHS does not depend on the choice).
+// when positive; otherwise face_zchunk_model with the device's resident
+// face blocks (SMs x the occupancy query's blocks per SM).
 int face_zchunk(const BoxDev &b, int zchunk, bool fp32);
+// Of 32, 16, 8, 6 and 4 planes, the one whose launch has the shortest
+// makespan when its blocks -- every full z block of every (x,y) tile, then
+// the short last z row -- are list-scheduled in launch order on `slots`
+// resident blocks, a block costing its planes plus its two lead-in planes
+// (ties keep the longer march).  Host only; the RHS does not depend on the
+// choice.
+int face_zchunk_model(int nx, int ny, int nz, int64_t slots);
 int64_t face_kernel_blocks(const BoxDev &b, int zchunk, bool fp32 = false);
 
 // T is the arithmetic type of the primitive cache, sources and RHS:

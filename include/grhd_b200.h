@@ -330,6 +330,16 @@ int grhd_eval_con2prim(grhd_ctx *ctx, int64_t n, const double *cons,
                        const double *gUU, double *prim, int *ok,
                        int *iterations, double *residual, void *stream);
 
+/* The face pass's z-march length (planes per block) for an nx x ny x nz
+ * interior on a device with `resident_blocks` face blocks resident at once
+ * (SMs x blocks per SM): of 32, 16, 8, 6 and 4 planes, the one whose blocks
+ * list-scheduled in launch order finish first, a block costing its planes
+ * plus two lead-in planes.  The kernels choose it this way whenever their
+ * caller gives no z-march length; the RHS does not depend on it.  Host
+ * only (no device call).  New (the reference has no face kernel). */
+int grhd_face_zchunk(int nx, int ny, int nz, int resident_blocks,
+                     int *zchunk);
+
 /* The FP64 division, reciprocal, square root and reciprocal square root
  * the kernels compute with, at n points: out[4n] = (a/b, 1/b, sqrt(a),
  * 1/sqrt(a)) per point (about one ulp from IEEE for normal operands and
