@@ -13,8 +13,9 @@ reference tree is available.  These tests check
   for bit (compute_rhs with its ghost fill, recover_primitives with its
   counters, compute_max_inverse_dt, advance_ssprk2, the error record of a
   failed recovery, the CCZ4-geometry operator) on the parity fixtures and
-  on two stressed tori (cells drained until their recovery fails; the
-  atmosphere dipped under its floors);
+  on three stressed tori (cells drained until their recovery fails; the
+  atmosphere dipped under its floors; cells sped up past the atmosphere's
+  velocity cap);
 * the reference RK4 the CPU baseline times (built from the operator's
   compute_rhs and update_conserved, one z slab per thread with the slab
   ghosts exchanged): independent of the slab count bit for bit, and equal
@@ -162,6 +163,27 @@ def _torus_atmosphere_dip():
     return p, box, s, t
 
 
+def _torus_fast():
+    """The a = 0.9 torus with the recovery's velocity cap at 0.9 and a
+    seeded fifth of its torus cells (rho > 1e-6) sped up to v^2 in
+    0.81..0.88 (v scaled, conserved variables rebuilt from the primitives;
+    v^2 = 1 - (rho / D)^2), above the atmosphere cap 0.8: the floors
+    rescale their velocities (6021 floored resets) and the face states
+    around them, and the RHS, CFL bound and SSPRK2 step go through."""
+    p, box, s, t = cases.CASES["torus_a09"]()
+    p.rec_max_velocity_squared = 0.9
+    v = O.state_view(box, s)
+    rng = np.random.default_rng(7)
+    v2 = 1.0 - (v[O.RHO] / v[O.D]) ** 2
+    sel = (v[O.RHO] > 1e-6) & (v2 > 1e-4) & (rng.random(v.shape[1:]) < 0.2)
+    target = rng.uniform(0.81, 0.88, v.shape[1:])
+    f = np.sqrt(np.where(sel, target / np.maximum(v2, 1e-300), 1.0))
+    for c in (O.V1, O.V2, O.V3):
+        v[c] = v[c] * f
+    O.fill_conserved_from_primitives(p, box, s, t)
+    return p, box, s, t
+
+
 def _cases():
     """The parity fixtures; the reference has no excision, so the cases
     that use it run here without it (their cells stay clear of the
@@ -171,7 +193,8 @@ def _cases():
               "michel_c1")]
     for name, make in named + [("torus_floors", _torus_floors),
                                ("torus_atmosphere_dip",
-                                _torus_atmosphere_dip)]:
+                                _torus_atmosphere_dip),
+                               ("torus_fast", _torus_fast)]:
         p, box, s, t = make()
         p.excision_radius = 0.0
         p.accretion_radius = 0.0
