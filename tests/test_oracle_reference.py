@@ -13,9 +13,9 @@ reference tree is available.  These tests check
   for bit (compute_rhs with its ghost fill, recover_primitives with its
   counters, compute_max_inverse_dt, advance_ssprk2, the error record of a
   failed recovery, the CCZ4-geometry operator) on the parity fixtures and
-  on three stressed tori (cells drained until their recovery fails; the
-  atmosphere dipped under its floors; cells sped up past the atmosphere's
-  velocity cap);
+  on stressed states (torus cells drained until their recovery fails; the
+  atmosphere of the torus and of the binary-PN disk dipped under its
+  floors; torus cells sped up past the atmosphere's velocity cap);
 * the reference RK4 the CPU baseline times (built from the operator's
   compute_rhs and update_conserved, one z slab per thread with the slab
   ghosts exchanged): independent of the slab count bit for bit, and equal
@@ -149,15 +149,16 @@ def _torus_floors():
     return p, box, s, t
 
 
-def _torus_atmosphere_dip():
-    """The a = 0.9 torus with every atmosphere cell (rho <= 2e-10) scaled
-    by 0.99 in all five conserved variables: their recovery converges at
-    the pressure floor and the floors raise rho back, so the floored-
-    primitive resets run (2304 interior cells) while the RHS, CFL bound
-    and SSPRK2 step go through."""
-    p, box, s, t = cases.CASES["torus_a09"]()
+def _atmosphere_dip(name):
+    """A parity fixture with every atmosphere cell (rho at most twice the
+    density floor) scaled by 0.99 in all five conserved variables: their
+    recovery converges at the pressure floor and the floors raise rho
+    back, so the floored-primitive resets run (the a = 0.9 torus: 2304
+    interior cells; the binary-PN disk, with its volume-time source:
+    27084) while the RHS, CFL bound and SSPRK2 step go through."""
+    p, box, s, t = cases.CASES[name]()
     v = O.state_view(box, s)
-    atm = v[O.RHO] <= 2e-10
+    atm = v[O.RHO] <= 2.0 * p.atmo_rho_floor
     for c in range(5):
         v[c] = np.where(atm, v[c] * 0.99, v[c])
     return p, box, s, t
@@ -193,7 +194,9 @@ def _cases():
               "michel_c1")]
     for name, make in named + [("torus_floors", _torus_floors),
                                ("torus_atmosphere_dip",
-                                _torus_atmosphere_dip),
+                                lambda: _atmosphere_dip("torus_a09")),
+                               ("pndisk_atmosphere_dip",
+                                lambda: _atmosphere_dip("pndisk")),
                                ("torus_fast", _torus_fast)]:
         p, box, s, t = make()
         p.excision_radius = 0.0
