@@ -273,11 +273,18 @@ def test_recovery_failure_record_equals_reference():
         (b.where, list(b.cell), b.residual)
 
 
-def test_ccz4_operator_equals_reference_bit_for_bit():
+@pytest.mark.parametrize("name", ["ksdisk", "ksdisk_atmosphere_dip",
+                                  "torus_fast"])
+def test_ccz4_operator_equals_reference_bit_for_bit(name):
     """LevelDataFiniteVolumeOperator (FArrayBoxFiniteVolume.hpp:1215-1364)
-    on the Kerr-Schild disk's state with the CCZ4 variables of its
-    background."""
-    p, box, s, t = cases.CASES["ksdisk"]()
+    on a state with the CCZ4 variables of its background: the Kerr-Schild
+    disk, the same with its atmosphere dipped under the floors, and the
+    torus with cells past the atmosphere's velocity cap."""
+    make = {"ksdisk": cases.CASES["ksdisk"],
+            "ksdisk_atmosphere_dip": lambda: _atmosphere_dip("ksdisk"),
+            "torus_fast": _torus_fast}[name]
+    p, box, s, t = make()
+    p.excision_radius = 0.0
     s36 = O.ccz4_state(p, box, s)
     a, b = s36.copy(), s36.copy()
     r_o = O.ccz4_compute_rhs(p, box, a)
@@ -291,11 +298,16 @@ def test_ccz4_operator_equals_reference_bit_for_bit():
     assert st == 0
     assert np.array_equal(r_o, r_r), np.abs(r_o - r_r).max()
     a, b = s36.copy(), s36.copy()
-    O.ccz4_recover_primitives(p, box, a)
+    d_o = O.ccz4_recover_primitives(p, box, a)
     d = O.Diag()
     L.ref_ccz4_recover_primitives(O.C.byref(p), O.C.byref(box), O._dp(b),
                                   O.C.byref(d))
     assert np.array_equal(a, b, equal_nan=True)
+    counts = (d.num_cells, d.num_failed_recoveries,
+              d.num_floored_primitives, d.num_conserved_resets)
+    assert counts == (d_o.num_cells, d_o.num_failed_recoveries,
+                      d_o.num_floored_primitives, d_o.num_conserved_resets)
+    print(name, "recovery counts", counts)
     out = O.C.c_double()
     L.ref_ccz4_compute_max_inverse_dt(O.C.byref(p), O.C.byref(box),
                                       O._dp(s36.copy()), O._dp(inv),
